@@ -1,0 +1,344 @@
+#!/usr/bin/env python
+"""Benchmark of the batched spline hot path (build + evaluate) on B200.
+
+Workload (default): the non-uniform quintic configuration -- degree-5 B-splines on 1024 cells with
+break points = uniform grid + U[-0.3h, 0.3h] noise, Hermite closures (derivative orders 1 and 2 at
+each end), 65536 batch lines in the (x, batch) layout, built from cos(2 pi k x + phi) samples and
+differentiated (first derivative) at 1024 random points per line. FP64 arithmetic.
+
+One step = one SplineBuilder call over all lines + one SplineEvaluator::deriv call over all lines.
+metric: Gpts/s = (lines * interpolation points + lines * evaluation points) / 2 / step time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun, one rank per GPU, every rank processing its own 65536 lines (weak
+scaling, no collective on the data path); time = max over ranks of the CUDA-event time.
+`--impl reference` times the reference algorithm's CPU restatement (oracle/, the reference's
+schedule: host factorisation, thread-per-line sweeps, OpenMP over lines) on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "spline build+eval Gpts/s & %HBM peak; FP64 vs FP32+refine at <=1e-12 rel err"
+UNIT = "Gpts/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--lines", type=int, default=1 << 16, help="batch lines per GPU")
+    p.add_argument("--e2e-steps", type=int, default=0, help="steps of the host-buffer (e2e) timing; 0 = --steps")
+    p.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU time of the baseline sample")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "100"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload_plan(D, lines):
+    from ddc_b200 import workloads
+
+    br = workloads.config2_breaks(1024)
+    bs = D.NonUniformBSplines(5, False, br)
+    pts = D.greville_points(bs, D.SplineBuilderClosure.HERMITE, D.SplineBuilderClosure.HERMITE)
+    return bs, pts, br
+
+
+def make_inputs(pts, lines, m, seed_offset=0):
+    from ddc_b200 import workloads
+
+    w = workloads.config2(B=lines, points=pts, m=m)
+    return w
+
+
+def algorithmic_bytes(lines, npts, nder, ncoef, m):
+    build = lines * (npts + nder) * 8 + lines * ncoef * 8
+    ev = lines * ncoef * 8 + lines * m * 8 * 2
+    return build, ev
+
+
+def cpu_reference_rate(lines_sample, seconds, threads=None):
+    """Time the oracle (reference schedule) on `lines_sample` lines: build + first-derivative eval."""
+    from oracle import oracle as O
+    from ddc_b200 import workloads
+
+    br = workloads.config2_breaks(1024)
+    obs = O.BSplines(5, False, breaks=br)
+    pts = obs.greville(O.HERMITE, O.HERMITE)
+    ob = O.Builder(obs, pts, O.HERMITE, O.HERMITE)
+    w = workloads.config2(B=lines_sample, points=pts, m=1024)
+    nt = threads or O.max_threads()
+    reps, t_total = 0, 0.0
+    t0 = time.perf_counter()
+    while True:
+        t1 = time.perf_counter()
+        c = ob(w["vals"], w["dlo"], w["dhi"], nthreads=nt)
+        O.evaluate(obs, w["coords"], c, order=1, nthreads=nt)
+        t_total += time.perf_counter() - t1
+        reps += 1
+        if time.perf_counter() - t0 > seconds:
+            break
+    pts_per_rep = lines_sample * (pts.size + 1024) / 2
+    return pts_per_rep * reps / t_total / 1e9, nt, reps, t_total
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    # each step is a bounded sample of the workload: 512 lines (of 65536) built and differentiated
+    from oracle import oracle as O
+
+    O.lib()
+    sample = 512
+    rates = []
+    for i in range(args.warmup + args.steps):
+        r, nt, reps, tt = cpu_reference_rate(sample, 0.0)
+        if i >= args.warmup:
+            rates.append(r)
+    value = float(np.median(rates))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "non-uniform quintic Hermite, 1024 cells, 65536 lines, build + d/dx at 1024 pts/line",
+                   "sample_lines_per_step": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nt, "kind": "port",
+                         "sample": f"{sample} lines per step (build + first-derivative eval), oracle/ restatement "
+                                   "of the reference's LAPACK path with its thread-per-line OpenMP schedule"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import ddc_b200 as D
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    lines, m = args.lines, 1024
+    bs, pts, br = workload_plan(D, lines)
+    builder = D.SplineBuilder(bs, pts, D.SplineBuilderClosure.HERMITE, D.SplineBuilderClosure.HERMITE)
+    ev = D.SplineEvaluator(bs)
+    w = make_inputs(pts, lines, m)
+    dev = torch.device("cuda", local)
+    h_vals = torch.from_numpy(w["vals"]).pin_memory()
+    h_dlo = torch.from_numpy(w["dlo"]).pin_memory()
+    h_dhi = torch.from_numpy(w["dhi"]).pin_memory()
+    h_x = torch.from_numpy(w["coords"]).pin_memory()
+    vals, dlo, dhi, x = (t.to(dev) for t in (h_vals, h_dlo, h_dhi, h_x))
+    coefs = torch.empty((bs.size, lines), dtype=torch.float64, device=dev)
+    out = torch.empty((m, lines), dtype=torch.float64, device=dev)
+    h_out = torch.empty((m, lines), dtype=torch.float64).pin_memory()
+    s = torch.cuda.current_stream()
+
+    def step():
+        builder(coefs, vals, dlo, dhi)
+        ev.deriv(1, out, x, coefs)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    # ---- device-resident timing (inputs > L2: 2.2 GB per step) ----
+    ev_b = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    ev_e = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(s)
+    for i in range(args.steps):
+        ev_b[i][0].record(s)
+        builder(coefs, vals, dlo, dhi)
+        ev_b[i][1].record(s)
+        ev_e[i][0].record(s)
+        ev.deriv(1, out, x, coefs)
+        ev_e[i][1].record(s)
+    t1.record(s)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = t0.elapsed_time(t1)
+    b_ms = float(np.mean([a.elapsed_time(b) for a, b in ev_b]))
+    e_ms = float(np.mean([a.elapsed_time(b) for a, b in ev_e]))
+    if world > 1:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    ms_step = ms / args.steps
+    npts = pts.size
+    total_pts = world * lines * (npts + m) / 2
+    value = total_pts / (ms_step * 1e-3) / 1e9
+    # ---- end-to-end through the public API with host buffers ----
+    ke = args.e2e_steps or args.steps
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(ke):
+        vals.copy_(h_vals, non_blocking=True)
+        dlo.copy_(h_dlo, non_blocking=True)
+        dhi.copy_(h_dhi, non_blocking=True)
+        x.copy_(h_x, non_blocking=True)
+        step()
+        h_out.copy_(out, non_blocking=True)
+    e1.record(s)
+    torch.cuda.synchronize()
+    e_ms_total = e0.elapsed_time(e1)
+    if world > 1:
+        tt = torch.tensor([e_ms_total], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e_ms_total = float(tt.item())
+    e2e_value = total_pts / (e_ms_total / ke * 1e-3) / 1e9
+    h2d = sum(t.numel() * 8 for t in (h_vals, h_dlo, h_dhi, h_x))
+    d2h = h_out.numel() * 8
+    # ---- roofline of the dominant kernel ----
+    b_bytes, e_bytes = algorithmic_bytes(lines, npts, 4, bs.size, m)
+    peak, peak_kind = peaks()
+    dom = "eval" if e_ms >= b_ms else "build"
+    dom_bytes, dom_ms = (e_bytes, e_ms) if dom == "eval" else (b_bytes, b_ms)
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            tr = json.load(f)
+        traffic = tr.get(dom)
+    except Exception:
+        pass
+    result = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu and world == 1:
+            try:
+                r, nt, reps, tt = cpu_reference_rate(256, args.cpu_seconds)
+                cpu = {"value": r, "unit": UNIT, "cores": nt, "kind": "port",
+                       "sample": f"256 of the 65536 lines (build + first-derivative eval at 1024 points), {reps} reps "
+                                 f"in {tt:.1f} s, oracle/ restatement of the reference's LAPACK path"}
+            except Exception as exc:  # the baseline is reported, not required
+                cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "port", "sample": f"failed: {exc}"}
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "non-uniform quintic Hermite B-splines, 1024 cells (1025 points + 2x2 derivatives), "
+                                   "65536 lines per GPU in (x, batch) layout, build + first derivative at 1024 random "
+                                   "points per line",
+                       "lines_per_gpu": lines, "degree": 5, "ncells": 1024, "eval_points_per_line": m,
+                       "l2": "inputs larger than L2 (2.2 GB touched per step)", "schedule": "two-call",
+                       "parallelism": f"batch-sharded x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "kernel": dom, "peak_kind": peak_kind},
+            "kernels": {"build_ms": b_ms, "eval_ms": e_ms,
+                        "build_GBps": b_bytes / (b_ms * 1e-3) / 1e9, "eval_GBps": e_bytes / (e_ms * 1e-3) / 1e9,
+                        "step_GBps": (b_bytes + e_bytes) / (ms_step * 1e-3) / 1e9},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": ke},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clk,
+        }
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

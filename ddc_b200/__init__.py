@@ -1,0 +1,19 @@
+"""B200-native batched spline builder / evaluator (DDC's SplineBuilder / SplineEvaluator hot path).
+
+The compute runs in hand-written sm_100a CUDA kernels inside libddcb.so, reached through the C-ABI
+of include/ddcb.h; this package is the host-side mirror of the reference's spline API.
+"""
+from . import _lib
+from ._lib import DdcbError
+from .splines import (BSplines, Extrapolation, NonUniformBSplines, SplineBuilder, SplineBuilderClosure,
+                      SplineEvaluator, UniformBSplines, greville_points, lines_of, n_boundary_equations)
+
+__all__ = [
+    "BSplines", "UniformBSplines", "NonUniformBSplines", "SplineBuilder", "SplineEvaluator", "SplineBuilderClosure",
+    "Extrapolation", "greville_points", "lines_of", "n_boundary_equations", "DdcbError", "load_library",
+]
+
+
+def load_library():
+    """Load libddcb.so (raises if it has not been built)."""
+    return _lib.load()

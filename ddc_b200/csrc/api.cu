@@ -1,0 +1,428 @@
+// api.cu -- the extern "C" boundary (include/ddcb.h). Each entry point validates its arguments,
+// runs the C++ plan / kernel code and turns every C++ exception into a ddcb_status.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "ddcb_internal.hpp"
+
+struct ddcb_bsplines_t
+{
+    ddcb::Basis basis;
+};
+struct ddcb_builder_t
+{
+    ddcb::Builder* b;
+};
+struct ddcb_evaluator_t
+{
+    ddcb::Evaluator* e;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <class F>
+ddcb_status guarded(F&& f)
+{
+    try {
+        f();
+        g_last_error.clear();
+        return DDCB_SUCCESS;
+    } catch (ddcb::Error const& e) {
+        g_last_error = e.what();
+        return e.status;
+    } catch (std::bad_alloc const&) {
+        g_last_error = "host allocation failed";
+        return DDCB_ERR_INVALID_ARGUMENT;
+    } catch (std::exception const& e) {
+        g_last_error = e.what();
+        return DDCB_ERR_INVALID_ARGUMENT;
+    }
+}
+
+void require(bool ok, char const* what)
+{
+    if (!ok) throw ddcb::Error(DDCB_ERR_INVALID_ARGUMENT, what);
+}
+
+void check_lines(ddcb_lines const& l, int64_t n_expected, char const* name)
+{
+    if (l.n != n_expected)
+        throw ddcb::Error(DDCB_ERR_INVALID_ARGUMENT, std::string(name) + ": extent along the interest dimension is "
+                                                           + std::to_string(l.n) + ", expected " + std::to_string(n_expected));
+    if (l.inner < 0 || l.outer < 0 || l.stride < 0 || l.outer_stride < 0)
+        throw ddcb::Error(DDCB_ERR_INVALID_ARGUMENT, std::string(name) + ": negative extent or stride");
+    if (l.inner * l.outer > 0 && l.n > 0 && l.stride == 0)
+        throw ddcb::Error(DDCB_ERR_INVALID_ARGUMENT, std::string(name) + ": zero stride along the interest dimension");
+    // 32-bit row index times stride must stay in 64-bit range; batch index fits in the grid
+    if (l.inner * l.outer > (int64_t(1) << 40)) throw ddcb::Error(DDCB_ERR_UNSUPPORTED, std::string(name) + ": too many lines");
+}
+
+void same_batch(ddcb_lines const& a, ddcb_lines const& b, char const* name)
+{
+    if (a.inner * a.outer != b.inner * b.outer)
+        throw ddcb::Error(DDCB_ERR_INVALID_ARGUMENT, std::string(name) + ": batch sizes differ");
+}
+
+} // namespace
+
+namespace ddcb {
+
+Evaluator* create_evaluator(Basis const& basis, int ex_lo, int ex_hi)
+{
+    auto* e = new Evaluator();
+    try {
+        e->basis.desc = basis.desc;
+        e->basis.knots = basis.knots;
+        e->basis.desc.knots = e->basis.knots.data();
+        e->ex_lo = ex_lo;
+        e->ex_hi = ex_hi;
+        BasisDesc const& D = e->basis.desc;
+        int const nk = int(e->basis.knots.size());
+        int const d = D.degree;
+        // knot-span inverses 1/(t[i+len]-t[i]) for len = 1..d (0 where the span is empty)
+        std::vector<double> inv(size_t(d) * nk, 0.0);
+        for (int len = 1; len <= d; ++len)
+            for (int i = 0; i + len < nk; ++i) {
+                double const s = e->basis.knots[i + len] - e->basis.knots[i];
+                inv[size_t(len - 1) * nk + i] = s > 0.0 ? 1.0 / s : 0.0;
+            }
+        // bucket table: the cell (knot index) holding the start of each of ncells uniform buckets
+        int const nb = std::max(1, D.ncells);
+        std::vector<int> lut(nb);
+        double const scale = double(nb) / (D.rmax - D.rmin);
+        int c = d;
+        for (int bk = 0; bk < nb; ++bk) {
+            double const x0 = D.rmin + double(bk) / scale;
+            while (c < d + D.ncells - 1 && x0 >= e->basis.knots[c + 1]) ++c;
+            lut[bk] = c;
+        }
+        e->integrals.resize(e->basis.size());
+        basis_integrals(e->basis, e->integrals.data());
+        int dev = 0;
+        DDCB_CUDA_CHECK(cudaGetDevice(&dev));
+        e->device = dev;
+        upload_basis(e->basis, dev);
+        size_t const b_inv = inv.size() * 8, b_lut = lut.size() * 4, b_int = e->integrals.size() * 8;
+        size_t const o_lut = (b_inv + 255) / 256 * 256, o_int = o_lut + (b_lut + 255) / 256 * 256;
+        size_t const total = o_int + b_int + 8;
+        DDCB_CUDA_CHECK(cudaMalloc(&e->d_block, total));
+        char* base = static_cast<char*>(e->d_block);
+        DDCB_CUDA_CHECK(cudaMemcpy(base, inv.data(), b_inv, cudaMemcpyHostToDevice));
+        DDCB_CUDA_CHECK(cudaMemcpy(base + o_lut, lut.data(), b_lut, cudaMemcpyHostToDevice));
+        DDCB_CUDA_CHECK(cudaMemcpy(base + o_int, e->integrals.data(), b_int, cudaMemcpyHostToDevice));
+        e->d_integrals = reinterpret_cast<double*>(base + o_int);
+        e->eb.b = e->basis.device_desc();
+        e->eb.inv_span = reinterpret_cast<double const*>(base);
+        e->eb.lut = reinterpret_cast<int const*>(base + o_lut);
+        e->eb.nbucket = nb;
+        e->eb.bucket_scale = scale;
+        e->eb.nk = nk;
+        return e;
+    } catch (...) {
+        destroy_evaluator(e);
+        throw;
+    }
+}
+
+void destroy_evaluator(Evaluator* e)
+{
+    if (!e) return;
+    if (e->d_block) cudaFree(e->d_block);
+    free_basis(e->basis);
+    delete e;
+}
+
+} // namespace ddcb
+
+extern "C" {
+
+const char* ddcb_status_string(ddcb_status s)
+{
+    switch (s) {
+    case DDCB_SUCCESS: return "success";
+    case DDCB_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case DDCB_ERR_BAD_GRID: return "invalid interpolation grid";
+    case DDCB_ERR_SINGULAR: return "singular matrix";
+    case DDCB_ERR_CUDA: return "CUDA error";
+    case DDCB_ERR_UNSUPPORTED: return "unsupported";
+    case DDCB_ERR_NOT_CONVERGED: return "not converged";
+    case DDCB_ERR_DEVICE: return "device-side failure";
+    }
+    return "unknown status";
+}
+
+const char* ddcb_last_error_message(void) { return g_last_error.c_str(); }
+
+ddcb_status ddcb_bsplines_create_uniform(int32_t degree, int32_t periodic, double rmin, double rmax, int64_t ncells,
+                                         ddcb_bsplines* out)
+{
+    return guarded([&] {
+        require(out != nullptr, "out is NULL");
+        auto* h = new ddcb_bsplines_t();
+        try {
+            ddcb::make_uniform_basis(h->basis, degree, periodic != 0, rmin, rmax, long(ncells));
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+ddcb_status ddcb_bsplines_create_non_uniform(int32_t degree, int32_t periodic, const double* breaks, int64_t nbreaks,
+                                             ddcb_bsplines* out)
+{
+    return guarded([&] {
+        require(out != nullptr, "out is NULL");
+        auto* h = new ddcb_bsplines_t();
+        try {
+            ddcb::make_non_uniform_basis(h->basis, degree, periodic != 0, breaks, long(nbreaks));
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+ddcb_status ddcb_bsplines_destroy(ddcb_bsplines b)
+{
+    return guarded([&] {
+        if (!b) return;
+        ddcb::free_basis(b->basis);
+        delete b;
+    });
+}
+
+ddcb_status ddcb_bsplines_get_info(ddcb_bsplines b, ddcb_bsplines_info* info)
+{
+    return guarded([&] {
+        require(b && info, "NULL argument");
+        auto const& d = b->basis.desc;
+        info->degree = d.degree;
+        info->periodic = d.periodic;
+        info->uniform = d.uniform;
+        info->ncells = d.ncells;
+        info->nbasis = b->basis.nbasis();
+        info->size = b->basis.size();
+        info->rmin = d.rmin;
+        info->rmax = d.rmax;
+    });
+}
+
+ddcb_status ddcb_bsplines_knots(ddcb_bsplines b, int64_t first, int64_t count, double* out)
+{
+    return guarded([&] {
+        require(b && out, "NULL argument");
+        require(first >= 0 && count >= 0 && first + count <= int64_t(b->basis.knots.size()), "knot range out of bounds");
+        std::copy(b->basis.knots.begin() + first, b->basis.knots.begin() + first + count, out);
+    });
+}
+
+ddcb_status ddcb_greville_points(ddcb_bsplines b, ddcb_closure lo, ddcb_closure hi, double* points, int64_t capacity,
+                                 int64_t* npoints)
+{
+    return guarded([&] {
+        require(b && npoints, "NULL argument");
+        auto pts = ddcb::greville_points(b->basis, int(lo), int(hi));
+        *npoints = int64_t(pts.size());
+        if (points) {
+            require(capacity >= int64_t(pts.size()), "capacity too small for the interpolation points");
+            std::copy(pts.begin(), pts.end(), points);
+        }
+    });
+}
+
+ddcb_status ddcb_bsplines_integrals(ddcb_bsplines b, double* out)
+{
+    return guarded([&] {
+        require(b && out, "NULL argument");
+        ddcb::basis_integrals(b->basis, out);
+    });
+}
+
+ddcb_status ddcb_builder_create(ddcb_bsplines basis, const double* interp_points, int64_t npoints, ddcb_closure lo,
+                                ddcb_closure hi, const ddcb_builder_options* options, ddcb_builder* out)
+{
+    return guarded([&] {
+        require(basis && out, "NULL argument");
+        auto* h = new ddcb_builder_t();
+        try {
+            h->b = ddcb::create_builder(basis->basis, interp_points, long(npoints), int(lo), int(hi), options);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+ddcb_status ddcb_builder_destroy(ddcb_builder b)
+{
+    return guarded([&] {
+        if (!b) return;
+        ddcb::destroy_builder(b->b);
+        delete b;
+    });
+}
+
+ddcb_status ddcb_builder_get_info(ddcb_builder h, ddcb_builder_info* info)
+{
+    return guarded([&] {
+        require(h && info, "NULL argument");
+        ddcb::Builder const& b = *h->b;
+        info->nbasis = b.n;
+        info->size = b.basis.size();
+        info->npoints = int64_t(b.points.size());
+        info->nbe_lo = b.nbe_lo;
+        info->nbe_hi = b.nbe_hi;
+        info->nbv_lo = b.nbv_lo;
+        info->nbv_hi = b.nbv_hi;
+        info->offset = b.offset;
+        info->dx = b.dx;
+        info->border = b.k;
+        info->kl = b.tables.kl;
+        info->ku = b.tables.ku;
+        info->pivoting = b.pivot;
+        info->chunks = b.tables.nchunk;
+        info->tile_lines = b.tile_lines;
+    });
+}
+
+ddcb_status ddcb_build(ddcb_builder h, double* coefs, ddcb_lines lc, const double* vals, ddcb_lines lv,
+                       const double* dlo, ddcb_lines llo, const double* dhi, ddcb_lines lhi, ddcb_stream stream)
+{
+    return guarded([&] {
+        require(h != nullptr, "builder is NULL");
+        ddcb::Builder const& b = *h->b;
+        check_lines(lv, int64_t(b.points.size()), "vals");
+        check_lines(lc, b.basis.size(), "coefs");
+        same_batch(lv, lc, "coefs/vals");
+        int64_t const nl = lv.inner * lv.outer;
+        if (nl == 0) return; // empty batch: nothing to do (spline_builder.hpp:929-931)
+        require(vals && coefs, "vals/coefs pointer is NULL");
+        if (b.lo == DDCB_HERMITE && b.nbv_lo > 0) {
+            require(dlo != nullptr, "derivs_lo is required by the lower HERMITE closure");
+            check_lines(llo, b.nbv_lo, "derivs_lo");
+            same_batch(llo, lv, "derivs_lo/vals");
+        } else {
+            dlo = nullptr;
+        }
+        if (b.hi == DDCB_HERMITE && b.nbv_hi > 0) {
+            require(dhi != nullptr, "derivs_hi is required by the upper HERMITE closure");
+            check_lines(lhi, b.nbv_hi, "derivs_hi");
+            same_batch(lhi, lv, "derivs_hi/vals");
+        } else {
+            dhi = nullptr;
+        }
+        int dev = 0;
+        DDCB_CUDA_CHECK(cudaGetDevice(&dev));
+        if (dev != b.device) throw ddcb::Error(DDCB_ERR_INVALID_ARGUMENT, "the builder was created for another device");
+        ddcb::launch_build(b, coefs, ddcb::to_lines(lc), vals, ddcb::to_lines(lv), dlo, ddcb::to_lines(llo), dhi,
+                           ddcb::to_lines(lhi), reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+ddcb_status ddcb_solve_multirhs(ddcb_builder h, double* rhs, int64_t ld, int64_t nrhs, int32_t transpose,
+                                ddcb_stream stream)
+{
+    return guarded([&] {
+        require(h != nullptr, "builder is NULL");
+        require(nrhs >= 0 && ld >= nrhs, "ld must be >= nrhs");
+        if (nrhs == 0) return;
+        require(rhs != nullptr, "rhs is NULL");
+        ddcb::launch_solve_multirhs(*h->b, rhs, long(ld), long(nrhs), transpose != 0, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+ddcb_status ddcb_quadrature_coefficients(ddcb_builder h, double* qlo, double* q, double* qhi)
+{
+    return guarded([&] {
+        require(h != nullptr, "builder is NULL");
+        ddcb::Builder const& b = *h->b;
+        require(q != nullptr, "q is NULL");
+        require(b.nbv_lo == 0 || qlo != nullptr, "q_derivs_lo is NULL");
+        require(b.nbv_hi == 0 || qhi != nullptr, "q_derivs_hi is NULL");
+        ddcb::builder_quadrature(b, qlo, q, qhi);
+    });
+}
+
+ddcb_status ddcb_evaluator_create(ddcb_bsplines basis, ddcb_extrapolation lo, ddcb_extrapolation hi, ddcb_evaluator* out)
+{
+    return guarded([&] {
+        require(basis && out, "NULL argument");
+        require(lo >= DDCB_EXTRAP_PERIODIC && lo <= DDCB_EXTRAP_CONSTANT && hi >= DDCB_EXTRAP_PERIODIC && hi <= DDCB_EXTRAP_CONSTANT,
+                "unknown extrapolation rule");
+        auto* h = new ddcb_evaluator_t();
+        try {
+            h->e = ddcb::create_evaluator(basis->basis, int(lo), int(hi));
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+ddcb_status ddcb_evaluator_destroy(ddcb_evaluator e)
+{
+    return guarded([&] {
+        if (!e) return;
+        ddcb::destroy_evaluator(e->e);
+        delete e;
+    });
+}
+
+static void eval_common(ddcb_evaluator h, int order, double* out, ddcb_lines lo, const double* coords, ddcb_lines lx,
+                        const double* coefs, ddcb_lines lc, ddcb_stream stream)
+{
+    require(h != nullptr, "evaluator is NULL");
+    ddcb::Evaluator const& e = *h->e;
+    check_lines(lc, e.basis.size(), "coefs");
+    check_lines(lx, lx.n, "coords");
+    check_lines(lo, lx.n, "out");
+    same_batch(lx, lo, "coords/out");
+    same_batch(lx, lc, "coords/coefs");
+    if (lx.inner * lx.outer == 0 || lx.n == 0) return;
+    require(out && coords && coefs, "NULL data pointer");
+    int dev = 0;
+    DDCB_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev != e.device) throw ddcb::Error(DDCB_ERR_INVALID_ARGUMENT, "the evaluator was created for another device");
+    ddcb::launch_eval(e, order, out, ddcb::to_lines(lo), coords, ddcb::to_lines(lx), coefs, ddcb::to_lines(lc),
+                      reinterpret_cast<cudaStream_t>(stream));
+}
+
+ddcb_status ddcb_eval(ddcb_evaluator h, double* out, ddcb_lines lo, const double* coords, ddcb_lines lx,
+                      const double* coefs, ddcb_lines lc, ddcb_stream stream)
+{
+    return guarded([&] { eval_common(h, 0, out, lo, coords, lx, coefs, lc, stream); });
+}
+
+ddcb_status ddcb_eval_deriv(ddcb_evaluator h, int32_t order, double* out, ddcb_lines lo, const double* coords,
+                            ddcb_lines lx, const double* coefs, ddcb_lines lc, ddcb_stream stream)
+{
+    return guarded([&] {
+        require(h != nullptr, "evaluator is NULL");
+        require(order >= 1 && order <= h->e->basis.desc.degree, "derivative order must be in 1..degree");
+        eval_common(h, order, out, lo, coords, lx, coefs, lc, stream);
+    });
+}
+
+ddcb_status ddcb_integrate(ddcb_evaluator h, double* out, int64_t out_outer_stride, const double* coefs, ddcb_lines lc,
+                           ddcb_stream stream)
+{
+    return guarded([&] {
+        require(h != nullptr, "evaluator is NULL");
+        ddcb::Evaluator const& e = *h->e;
+        check_lines(lc, e.basis.size(), "coefs");
+        if (lc.inner * lc.outer == 0) return;
+        require(out && coefs, "NULL data pointer");
+        ddcb::launch_integrate(e, out, out_outer_stride, coefs, ddcb::to_lines(lc), reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+} // extern "C"

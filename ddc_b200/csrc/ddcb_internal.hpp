@@ -1,0 +1,162 @@
+// ddcb_internal.hpp -- host-side plan objects and the kernel parameter blocks.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/ddcb.h"
+#include "bspline_math.cuh"
+#include "eval_device.cuh"
+
+namespace ddcb {
+
+// An error carrying a ddcb_status across the C++ layers up to the C-ABI boundary.
+struct Error : std::runtime_error
+{
+    ddcb_status status;
+    Error(ddcb_status s, std::string const& msg) : std::runtime_error(msg), status(s) {}
+};
+
+#define DDCB_CUDA_CHECK(expr)                                                                      \
+    do {                                                                                           \
+        cudaError_t const e_ = (expr);                                                             \
+        if (e_ != cudaSuccess)                                                                     \
+            throw ::ddcb::Error(DDCB_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// Strided batched array view: element (i, b) at base[i*stride + (b/inner)*outer_stride + b%inner].
+struct Lines
+{
+    int64_t n, stride, inner, outer, outer_stride;
+    int64_t nlines() const { return inner * outer; }
+};
+
+inline Lines to_lines(ddcb_lines const& l) { return Lines {l.n, l.stride, l.inner, l.outer, l.outer_stride}; }
+
+// Device-side description of the banded solve of one builder (all pointers are device pointers).
+//
+// The system A (size n) is split as [[Q, g],[l, S0]] with a border of k rows/cols (periodic corner
+// coupling); Q (size m = n - k) is factored P Q = L U with partial pivoting. L has kl
+// sub-diagonals, U has ku super-diagonals (after pivoting fill-in). Each line is solved by
+// NC chunk threads (three-phase chunked sweeps with carries, see build_kernels.cu).
+struct SolveTables
+{
+    int n, m, k;
+    int kl, ku;
+    int pivot;       // 1 if any row interchange happened
+    int nchunk;      // chunks per line used by the sweeps
+    int chunk_len;   // every chunk but the last has this (odd) length; the last absorbs the rest
+    const double* Lf;    // m x kl: Lf[j*kl + t-1] = multiplier of row j+t at step j
+    const int8_t* piv;   // m: pivot row offset at step j (ipiv[j] - j)
+    const double* Uf;    // m x (ku+1): [1/U_jj, U_j,j+1 .. U_j,j+ku]
+    const double* PhiF;  // nchunk x kl x kl forward carry transfer
+    const double* PhiB;  // nchunk x ku x ku backward carry transfer
+    // border (k > 0)
+    int lam_nnz;
+    const int* lam_row;
+    const int* lam_col;
+    const double* lam_val;
+    const double* Sinv;  // k x k inverse of the Schur complement S0 - l Q^-1 g
+    int qg_lo, qg_hi;    // rows [0, qg_lo) and [m - qg_hi, m) of Q^-1 g are kept (rest < 1e-19)
+    const double* Qg;    // (qg_lo + qg_hi) x k
+};
+
+// How the right-hand side rows are gathered from the inputs and how the coefficients are placed.
+struct RhsMap
+{
+    int nbe_lo, nbe_hi;   // Hermite rows at each end
+    int nbv_lo, nbv_hi;   // of which read from the derivative inputs (0 for homogeneous Hermite)
+    int npoints;          // interpolation values
+    int offset;           // periodic column rotation (spline_builder.hpp:619-658)
+    int size;             // coefficient rows (nbasis + degree)
+    int periodic;
+    double dxpow_lo[8];   // dx^(i+odd) for the Hermite rows
+    double dxpow_hi[8];
+};
+
+struct Basis
+{
+    BasisDesc desc {};          // desc.knots points at host knots
+    std::vector<double> knots;  // non-uniform knots (host)
+    int device = -1;
+    double* d_knots = nullptr;  // device copy of knots
+    BasisDesc device_desc() const
+    {
+        BasisDesc d = desc;
+        d.knots = d_knots;
+        return d;
+    }
+    long nbasis() const { return desc.ncells + (desc.periodic ? 0 : desc.degree); }
+    long size() const { return desc.ncells + desc.degree; }
+};
+
+struct Builder
+{
+    Basis basis;            // own copy of the basis (knots uploaded for this builder's device)
+    int lo = 0, hi = 0;
+    int nbe_lo = 0, nbe_hi = 0, nbv_lo = 0, nbv_hi = 0, odd = 0;
+    int offset = 0;
+    double dx = 0.0;
+    long n = 0;             // nbasis
+    std::vector<double> points;
+    std::vector<double> A;  // assembled dense matrix (n x n), kept for the adjoint / checks
+    int precision = DDCB_FP64;
+    int refine_rounds = 2;
+    int device = -1;
+    int tile_lines = 8;     // lines per CTA
+    int nchunk_req = 32;    // requested chunks per line
+    // host copies of the solve tables (for quadrature / transposed host solves)
+    int k = 0, m = 0, kl = 0, ku = 0, pivot = 0;
+    std::vector<double> lu_band;   // factored Q
+    std::vector<int> ipiv;
+    SolveTables tables {};         // device pointers
+    SolveTables tables_t {};       // tables of A^T (adjoint)
+    float* tables_f32 = nullptr;   // FP32 copies (refinement mode)
+    void* d_block = nullptr;       // one allocation holding every device table
+    size_t d_block_bytes = 0;
+    RhsMap rhs {};
+    std::string structure;
+    void* host_private = nullptr;  // host factorisation (plan.cpp)
+};
+
+struct Evaluator
+{
+    Basis basis;
+    int ex_lo = DDCB_EXTRAP_NULL, ex_hi = DDCB_EXTRAP_NULL;
+    int device = -1;
+    EvalBasis eb {};               // device view: knots, knot-span inverses, cell lookup table
+    double* d_integrals = nullptr; // integrals of the B-splines (size entries), inside d_block
+    void* d_block = nullptr;
+    std::vector<double> integrals;
+};
+
+Evaluator* create_evaluator(Basis const& basis, int ex_lo, int ex_hi);
+void destroy_evaluator(Evaluator* e);
+
+// plan.cpp
+void make_uniform_basis(Basis& b, int degree, bool periodic, double rmin, double rmax, long ncells);
+void make_non_uniform_basis(Basis& b, int degree, bool periodic, double const* breaks, long nbreaks);
+void upload_basis(Basis& b, int device);
+void free_basis(Basis& b);
+std::vector<double> greville_points(Basis const& b, int lo, int hi);
+void basis_integrals(Basis const& b, double* out);
+Builder* create_builder(Basis const& basis, double const* pts, long npts, int lo, int hi, ddcb_builder_options const* opts);
+void destroy_builder(Builder* b);
+void builder_quadrature(Builder const& b, double* qlo, double* q, double* qhi);
+
+// build_kernels.cu
+void launch_build(Builder const& b, double* coefs, Lines const& lc, double const* vals, Lines const& lv,
+                  double const* dlo, Lines const& llo, double const* dhi, Lines const& lhi, cudaStream_t s);
+void launch_solve_multirhs(Builder const& b, double* rhs, long ld, long nrhs, bool transpose, cudaStream_t s);
+
+// eval_kernels.cu
+void launch_eval(Evaluator const& e, int order, double* out, Lines const& lo, double const* coords, Lines const& lx,
+                 double const* coefs, Lines const& lc, cudaStream_t s);
+void launch_integrate(Evaluator const& e, double* out, int64_t out_stride, double const* coefs, Lines const& lc,
+                      cudaStream_t s);
+
+} // namespace ddcb

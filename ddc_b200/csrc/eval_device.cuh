@@ -1,0 +1,121 @@
+// eval_device.cuh -- device-side point evaluation of a spline from a coefficient tile.
+#pragma once
+
+#include "bspline_math.cuh"
+
+namespace ddcb {
+
+// Everything the kernels need to locate a point and evaluate the basis.
+struct EvalBasis
+{
+    BasisDesc b;              // b.knots: device knots (or a shared-memory copy inside a kernel)
+    const double* inv_span;   // degree x nk: inv_span[(len-1)*nk + i] = 1/(t[i+len]-t[i]) (0 if empty)
+    const int* lut;           // nbucket entries: knot index of the cell holding each bucket start
+    int nbucket;
+    double bucket_scale;      // nbucket / (rmax - rmin)
+    int nk;                   // number of knots
+};
+
+#if defined(__CUDACC__)
+
+// Cell of x as a knot index (the cell [t_c, t_c+1) with t_c <= x < t_c+1), with the end rules of
+// bsplines_non_uniform.hpp:666-695. A bucket table gives a starting cell; short walks finish it,
+// so the result equals the bisection's for any mesh.
+__device__ __forceinline__ int nonuniform_locate(EvalBasis const& eb, double x)
+{
+    int const d = eb.b.degree;
+    int const last = d + eb.b.ncells - 1;
+    if (x <= eb.b.rmin) return d;
+    if (x >= eb.b.rmax) return last;
+    int bk = static_cast<int>((x - eb.b.rmin) * eb.bucket_scale);
+    bk = bk < 0 ? 0 : (bk >= eb.nbucket ? eb.nbucket - 1 : bk);
+    int c = __ldg(eb.lut + bk);
+    double const* K = eb.b.knots;
+    while (c < last && x >= K[c + 1]) ++c;
+    while (c > d && x < K[c]) --c;
+    return c;
+}
+
+// s(x) without boundary handling (spline_evaluator.hpp:556-605). C[i*cs] is the coefficient of
+// B-spline i.
+template <int D, bool UNI>
+__device__ __forceinline__ double eval_value_no_bc(EvalBasis const& eb, double x, const double* C, int cs)
+{
+    double v[D + 1];
+    int jmin;
+    if (UNI) {
+        double off;
+        jmin = uniform_cell(eb.b, x, off);
+        uniform_values_t<D>(off, v);
+    } else {
+        int const ck = nonuniform_locate(eb, x);
+        nonuniform_values_t<D>(eb.b.knots, eb.inv_span, eb.nk, ck, x, v);
+        jmin = ck - D;
+    }
+    double y = 0.0;
+#pragma unroll
+    for (int i = 0; i < D + 1; ++i) y = fma(C[(jmin + i) * cs], v[i], y);
+    return y;
+}
+
+// s(x) with the periodic wrap or the extrapolation rules (spline_evaluator.hpp:529-554,
+// null_extrapolation_rule.hpp:14-26, constant_extrapolation_rule.hpp:27-52 evaluated at the
+// domain end).
+template <int D, bool UNI>
+__device__ __forceinline__ double eval_value_bc(EvalBasis const& eb, int ex_lo, int ex_hi, double x, const double* C, int cs)
+{
+    if (eb.b.periodic) {
+        x = periodic_wrap(eb.b, x);
+    } else {
+        if (x < eb.b.rmin) {
+            if (ex_lo == 1) return 0.0;
+            x = eb.b.rmin;
+        } else if (x > eb.b.rmax) {
+            if (ex_hi == 1) return 0.0;
+            x = eb.b.rmax;
+        }
+    }
+    return eval_value_no_bc<D, UNI>(eb, x, C, cs);
+}
+
+// d^ORDER s / dx^ORDER at x (spline_evaluator.hpp:388-430, no boundary handling): ORDER rounds of
+// divided differences of the d+1 coefficients of the cell, then the degree-(D-ORDER) basis.
+template <int D, int ORDER, bool UNI>
+__device__ __forceinline__ double eval_deriv_no_bc(EvalBasis const& eb, double x, const double* C, int cs)
+{
+    constexpr int P = D - ORDER;
+    double cc[D + 1];
+    double v[P + 1];
+    int jmin;
+    if (UNI) {
+        double off;
+        jmin = uniform_cell(eb.b, x, off);
+        uniform_values_t<P>(off, v);
+    } else {
+        int const ck = nonuniform_locate(eb, x);
+        nonuniform_values_t<P>(eb.b.knots, eb.inv_span, eb.nk, ck, x, v);
+        jmin = ck - D;
+    }
+#pragma unroll
+    for (int i = 0; i < D + 1; ++i) cc[i] = C[(jmin + i) * cs];
+#pragma unroll
+    for (int k = 1; k <= ORDER; ++k) {
+#pragma unroll
+        for (int i = D; i >= k; --i) {
+            if (UNI) {
+                cc[i] = (cc[i] - cc[i - 1]) * eb.b.inv_step;
+            } else {
+                // c^(k)_j = (D-k+1) (c_j - c_{j-1}) / (t_{j+D-k+1} - t_j), j = jmin + i
+                cc[i] = double(D - k + 1) * (cc[i] - cc[i - 1]) * __ldg(eb.inv_span + (D - k) * eb.nk + jmin + i);
+            }
+        }
+    }
+    double y = 0.0;
+#pragma unroll
+    for (int r = 0; r < P + 1; ++r) y = fma(cc[ORDER + r], v[r], y);
+    return y;
+}
+
+#endif // __CUDACC__
+
+} // namespace ddcb

@@ -1,0 +1,157 @@
+// eval_kernels.cu -- batched spline evaluation, differentiation and integration
+// (SplineEvaluator::operator(), ::deriv, ::integrate; spline_evaluator.hpp:257-526).
+//
+// A thread block owns TLE batch lines: it stages their coefficient rows in shared memory once
+// (coalesced over the contiguous batch dimension) and then evaluates every point of those lines,
+// gathering the degree+1 coefficients of each point from shared memory. The basis values are
+// computed in registers with the degree known at compile time. Derivatives of order n use the
+// derivative spline: n rounds of divided differences of the coefficients (de Boor, "A Practical
+// Guide to Splines", X.(15)) followed by the degree-(d-n) basis, which needs no division on device
+// (the knot-span inverses come from a table built with the evaluator).
+#include <algorithm>
+
+#include "ddcb_internal.hpp"
+#include "eval_device.cuh"
+
+namespace ddcb {
+
+namespace {
+
+struct EvalArgs
+{
+    EvalBasis eb;
+    int ex_lo, ex_hi;
+    int64_t nlines;
+    int size;           // coefficient rows
+    const double* coords;
+    Lines lx;
+    const double* coefs;
+    Lines lc;
+    double* out;
+    Lines lo;
+};
+
+__device__ __forceinline__ int64_t line_offset(Lines const& L, int64_t b)
+{
+    return (b / L.inner) * L.outer_stride + (b % L.inner);
+}
+
+template <int D, int TLE, int ORDER, bool UNI>
+__global__ void __launch_bounds__(256) eval_kernel(const __grid_constant__ EvalArgs a)
+{
+    extern __shared__ double smem[];
+    double* C = smem;                                  // size x TLE coefficient tile
+    double* K = C + (size_t)a.size * TLE;              // knots (non-uniform)
+    int const tid = threadIdx.x;
+    int const l = tid % TLE;
+    int const c = tid / TLE;
+    int const nct = blockDim.x / TLE;
+    int64_t const line = (int64_t)blockIdx.x * TLE + l;
+    bool const live = line < a.nlines;
+    if (live) {
+        int64_t const oc = line_offset(a.lc, line);
+        for (int r = c; r < a.size; r += nct) C[r * TLE + l] = a.coefs[r * a.lc.stride + oc];
+    }
+    if (!UNI)
+        for (int i = tid; i < a.eb.nk; i += blockDim.x) K[i] = a.eb.b.knots[i];
+    __syncthreads();
+    if (!live) return;
+    EvalBasis eb = a.eb;
+    if (!UNI) eb.b.knots = K;
+    int64_t const ox = line_offset(a.lx, line);
+    int64_t const oo = line_offset(a.lo, line);
+    int64_t const m = a.lx.n;
+    for (int64_t p = c; p < m; p += nct) {
+        double const x = a.coords[p * a.lx.stride + ox];
+        double y;
+        if (ORDER == 0) y = eval_value_bc<D, UNI>(eb, a.ex_lo, a.ex_hi, x, C + l, TLE);
+        else y = eval_deriv_no_bc<D, ORDER, UNI>(eb, x, C + l, TLE);
+        a.out[p * a.lo.stride + oo] = y;
+    }
+}
+
+template <int D, int TLE, bool UNI>
+void launch_order(EvalArgs const& a, int order, size_t sm, cudaStream_t s)
+{
+    dim3 grid((unsigned)((a.nlines + TLE - 1) / TLE)), block(256);
+#define DDCB_EVAL_CASE(O)                                                                                  \
+    case O:                                                                                                \
+        if constexpr (O <= D) {                                                                            \
+            auto k = eval_kernel<D, TLE, O, UNI>;                                                          \
+            if (sm > 48 * 1024) DDCB_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm))); \
+            k<<<grid, block, sm, s>>>(a);                                                                  \
+        }                                                                                                  \
+        break;
+    switch (order) {
+        DDCB_EVAL_CASE(0)
+        DDCB_EVAL_CASE(1)
+        DDCB_EVAL_CASE(2)
+        DDCB_EVAL_CASE(3)
+        DDCB_EVAL_CASE(4)
+        DDCB_EVAL_CASE(5)
+    default: break;
+    }
+#undef DDCB_EVAL_CASE
+    DDCB_CUDA_CHECK(cudaGetLastError());
+}
+
+template <int TLE>
+void launch_deg(EvalArgs const& a, int order, size_t sm, cudaStream_t s)
+{
+    bool const uni = a.eb.b.uniform != 0;
+    switch (a.eb.b.degree) {
+    case 1: uni ? launch_order<1, TLE, true>(a, order, sm, s) : launch_order<1, TLE, false>(a, order, sm, s); break;
+    case 2: uni ? launch_order<2, TLE, true>(a, order, sm, s) : launch_order<2, TLE, false>(a, order, sm, s); break;
+    case 3: uni ? launch_order<3, TLE, true>(a, order, sm, s) : launch_order<3, TLE, false>(a, order, sm, s); break;
+    case 4: uni ? launch_order<4, TLE, true>(a, order, sm, s) : launch_order<4, TLE, false>(a, order, sm, s); break;
+    case 5: uni ? launch_order<5, TLE, true>(a, order, sm, s) : launch_order<5, TLE, false>(a, order, sm, s); break;
+    default: throw Error(DDCB_ERR_UNSUPPORTED, "degree must be in 1..5");
+    }
+}
+
+__global__ void integrate_kernel(const double* __restrict__ coefs, Lines lc, const double* __restrict__ ints, int size,
+                                 double* __restrict__ out, int64_t out_outer_stride, int64_t nlines)
+{
+    int64_t const line = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (line >= nlines) return;
+    int64_t const oc = line_offset(lc, line);
+    double s = 0.0;
+    for (int i = 0; i < size; ++i) s = fma(coefs[i * lc.stride + oc], __ldg(ints + i), s);
+    out[(line / lc.inner) * out_outer_stride + line % lc.inner] = s;
+}
+
+} // namespace
+
+void launch_eval(Evaluator const& e, int order, double* out, Lines const& lo, double const* coords, Lines const& lx,
+                 double const* coefs, Lines const& lc, cudaStream_t s)
+{
+    EvalArgs a {};
+    a.eb = e.eb;
+    a.ex_lo = e.ex_lo;
+    a.ex_hi = e.ex_hi;
+    a.nlines = lx.nlines();
+    a.size = int(e.basis.size());
+    a.coords = coords;
+    a.lx = lx;
+    a.coefs = coefs;
+    a.lc = lc;
+    a.out = out;
+    a.lo = lo;
+    if (a.nlines == 0 || lx.n == 0) return;
+    constexpr int TLE = 8;
+    size_t sm = sizeof(double) * ((size_t)a.size * TLE + (e.eb.b.uniform ? 0 : (size_t)e.eb.nk));
+    launch_deg<TLE>(a, order, sm, s);
+}
+
+void launch_integrate(Evaluator const& e, double* out, int64_t out_outer_stride, double const* coefs, Lines const& lc,
+                      cudaStream_t s)
+{
+    int64_t const nl = lc.nlines();
+    if (nl == 0) return;
+    int const bs = 256;
+    integrate_kernel<<<dim3((unsigned)((nl + bs - 1) / bs)), dim3(bs), 0, s>>>(coefs, lc, e.d_integrals, int(e.basis.size()),
+                                                                              out, out_outer_stride, nl);
+    DDCB_CUDA_CHECK(cudaGetLastError());
+}
+
+} // namespace ddcb

@@ -1,0 +1,274 @@
+"""Host-side mirror of DDC's spline API (src/ddc/kernels/splines/) over the C-ABI.
+
+Class and argument names follow the reference: UniformBSplines / NonUniformBSplines
+(bsplines_uniform.hpp, bsplines_non_uniform.hpp), GrevilleInterpolationPoints
+(greville_interpolation_points.hpp), SplineBuilder (spline_builder.hpp) and SplineEvaluator
+(spline_evaluator.hpp). Batched data are CUDA tensors (the reference's ChunkSpans in a device
+memory space); the dimension of interest is given by `dim`, every other dimension is a batch
+dimension, in any order (the reference's 1DX / 2DXB1 / 2DB1X ... layouts).
+
+Errors follow the reference: invalid grids raise RuntimeError with the reference's messages
+(check_valid_grid), and every failing C call raises ddc_b200._lib.DdcbError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import (EXTRAP_CONSTANT, EXTRAP_NULL, EXTRAP_PERIODIC, FP32_REFINE, FP64, GREVILLE, HERMITE,
+                   HOMOGENEOUS_HERMITE, PERIODIC, BuilderInfo, BuilderOptions, BSplinesInfo, Lines)
+
+
+class SplineBuilderClosure:
+    """ddc::SplineBuilderClosure (spline_builder_closures.hpp:18-23)."""
+
+    PERIODIC = PERIODIC
+    HERMITE = HERMITE
+    HOMOGENEOUS_HERMITE = HOMOGENEOUS_HERMITE
+    GREVILLE = GREVILLE
+
+
+class Extrapolation:
+    PERIODIC = EXTRAP_PERIODIC
+    NULL = EXTRAP_NULL
+    CONSTANT = EXTRAP_CONSTANT
+
+
+def n_boundary_equations(closure: int, degree: int) -> int:
+    """spline_builder_closures.hpp:43-55."""
+    return degree // 2 if closure in (HERMITE, HOMOGENEOUS_HERMITE) else 0
+
+
+def _stream_handle(stream):
+    import torch
+
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
+
+
+def lines_of(t, dim: int) -> Lines:
+    """ddcb_lines of tensor `t` with interest dimension `dim`; batch = all other dims (row-major)."""
+    shape = list(t.shape)
+    stride = list(t.stride())
+    nd = len(shape)
+    dim = dim % nd if nd else 0
+    n = shape[dim] if nd else 1
+    inner_dims = list(range(dim + 1, nd))
+    outer_dims = list(range(0, dim))
+    inner = math.prod(shape[d] for d in inner_dims)
+    outer = math.prod(shape[d] for d in outer_dims)
+    exp = 1
+    for d in reversed(inner_dims):
+        if shape[d] > 1 and stride[d] != exp:
+            raise ValueError("the batch dimensions after the interest dimension must be contiguous")
+        exp *= shape[d]
+    os_ = 0
+    if outer_dims:
+        os_ = stride[outer_dims[-1]] if shape[outer_dims[-1]] > 1 else 0
+        exp = os_
+        for d in reversed(outer_dims):
+            if shape[d] > 1 and stride[d] != exp:
+                raise ValueError("the batch dimensions before the interest dimension must be regularly strided")
+            exp *= shape[d]
+    return Lines(n, stride[dim] if nd else 1, inner, outer, os_)
+
+
+def _ptr(t):
+    return C.c_void_p(0 if t is None else t.data_ptr())
+
+
+def _dev_f64(t, name):
+    import torch
+
+    if t is None:
+        return None
+    if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float64):
+        raise TypeError(f"{name} must be a CUDA float64 tensor")
+    return t
+
+
+class BSplines:
+    """A B-spline basis: UniformBSplines<CDim, D>::Impl or NonUniformBSplines<CDim, D>::Impl."""
+
+    def __init__(self, degree: int, periodic: bool, *, rmin=None, rmax=None, ncells=None, breaks=None):
+        h = C.c_void_p()
+        if breaks is None:
+            _lib.call("ddcb_bsplines_create_uniform", int(degree), int(bool(periodic)), float(rmin), float(rmax),
+                      int(ncells), C.byref(h))
+        else:
+            b = np.ascontiguousarray(breaks, dtype=np.float64)
+            _lib.call("ddcb_bsplines_create_non_uniform", int(degree), int(bool(periodic)),
+                      b.ctypes.data_as(C.c_void_p), b.size, C.byref(h))
+        self._h = h
+        info = BSplinesInfo()
+        _lib.call("ddcb_bsplines_get_info", h, C.byref(info))
+        self.degree = info.degree
+        self.periodic = bool(info.periodic)
+        self.uniform = bool(info.uniform)
+        self.ncells = info.ncells
+        self.nbasis = info.nbasis
+        self.size = info.size
+        self.rmin = info.rmin
+        self.rmax = info.rmax
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.load().ddcb_bsplines_destroy(h)
+            self._h = None
+
+    @property
+    def length(self):
+        return self.rmax - self.rmin
+
+    def knots(self) -> np.ndarray:
+        n = self.ncells + 1 + 2 * self.degree
+        out = np.zeros(n)
+        _lib.call("ddcb_bsplines_knots", self._h, 0, n, out.ctypes.data_as(C.c_void_p))
+        return out
+
+    def integrals(self) -> np.ndarray:
+        """integrals() of integrals.hpp:165-177: one value per B-spline (size() entries)."""
+        out = np.zeros(self.size)
+        _lib.call("ddcb_bsplines_integrals", self._h, out.ctypes.data_as(C.c_void_p))
+        return out
+
+
+def UniformBSplines(degree, periodic, rmin, rmax, ncells) -> BSplines:
+    return BSplines(degree, periodic, rmin=rmin, rmax=rmax, ncells=ncells)
+
+
+def NonUniformBSplines(degree, periodic, breaks) -> BSplines:
+    return BSplines(degree, periodic, breaks=breaks)
+
+
+def greville_points(bsplines: BSplines, lower: int, upper: int) -> np.ndarray:
+    """GrevilleInterpolationPoints<BSplines, lower, upper>::get_sampling() coordinates."""
+    n = C.c_int64()
+    _lib.call("ddcb_greville_points", bsplines._h, int(lower), int(upper), None, 0, C.byref(n))
+    out = np.zeros(n.value)
+    _lib.call("ddcb_greville_points", bsplines._h, int(lower), int(upper), out.ctypes.data_as(C.c_void_p), out.size,
+              C.byref(n))
+    return out
+
+
+class SplineBuilder:
+    """ddc::SplineBuilder with the B200 solver: operator() builds spline coefficients on the GPU."""
+
+    def __init__(self, bsplines: BSplines, interpolation_points: Optional[Sequence[float]] = None,
+                 lower: int = GREVILLE, upper: int = GREVILLE, *, precision: str = "fp64", refine_rounds: int = 2,
+                 tile_lines: int = 0, chunks: int = 0):
+        if bsplines.periodic:
+            lower = upper = PERIODIC
+        self.bsplines = bsplines
+        self.lower, self.upper = lower, upper
+        if interpolation_points is None:
+            interpolation_points = greville_points(bsplines, lower, upper)
+        pts = np.ascontiguousarray(interpolation_points, dtype=np.float64)
+        self.interpolation_points = pts
+        opts = BuilderOptions(FP32_REFINE if precision == "fp32_refine" else FP64, int(refine_rounds),
+                              int(tile_lines), int(chunks))
+        h = C.c_void_p()
+        _lib.call("ddcb_builder_create", bsplines._h, pts.ctypes.data_as(C.c_void_p), pts.size, int(lower),
+                  int(upper), C.byref(opts), C.byref(h))
+        self._h = h
+        info = BuilderInfo()
+        _lib.call("ddcb_builder_get_info", h, C.byref(info))
+        self.info = info
+        self.s_nbe_xmin, self.s_nbe_xmax = info.nbe_lo, info.nbe_hi
+        self.s_nbv_xmin, self.s_nbv_xmax = info.nbv_lo, info.nbv_hi
+        self.s_odd = bsplines.degree % 2
+        self.offset = info.offset
+        self.dx = info.dx
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.load().ddcb_builder_destroy(h)
+            self._h = None
+
+    @property
+    def npoints(self):
+        return self.info.npoints
+
+    def __call__(self, spline, vals, derivs_xmin=None, derivs_xmax=None, *, dim: int = 0, stream=None):
+        """SplineBuilder::operator()(spline, vals, derivs_xmin, derivs_xmax) (spline_builder.hpp:896-1101)."""
+        spline = _dev_f64(spline, "spline")
+        vals = _dev_f64(vals, "vals")
+        dlo = _dev_f64(derivs_xmin, "derivs_xmin")
+        dhi = _dev_f64(derivs_xmax, "derivs_xmax")
+        lc, lv = lines_of(spline, dim), lines_of(vals, dim)
+        llo = lines_of(dlo, dim) if dlo is not None else Lines(0, 1, 0, 0, 0)
+        lhi = lines_of(dhi, dim) if dhi is not None else Lines(0, 1, 0, 0, 0)
+        _lib.call("ddcb_build", self._h, _ptr(spline), lc, _ptr(vals), lv, _ptr(dlo), llo, _ptr(dhi), lhi,
+                  _stream_handle(stream))
+        return spline
+
+    def solve(self, rhs, transpose: bool = False, stream=None):
+        """In-place SplinesLinearProblem::solve on a (nbasis, nrhs) CUDA float64 matrix."""
+        rhs = _dev_f64(rhs, "rhs")
+        assert rhs.ndim == 2 and rhs.shape[0] == self.info.nbasis and rhs.stride(1) == 1
+        _lib.call("ddcb_solve_multirhs", self._h, _ptr(rhs), rhs.stride(0), rhs.shape[1], int(transpose),
+                  _stream_handle(stream))
+        return rhs
+
+    def quadrature_coefficients(self):
+        """quadrature_coefficients() (spline_builder.hpp:1103-1234): (q_derivs_xmin, q, q_derivs_xmax)."""
+        nb = self.info.nbasis
+        qlo = np.zeros(max(self.s_nbv_xmin, 1))
+        q = np.zeros(nb - self.s_nbv_xmin - self.s_nbv_xmax)
+        qhi = np.zeros(max(self.s_nbv_xmax, 1))
+        _lib.call("ddcb_quadrature_coefficients", self._h, qlo.ctypes.data_as(C.c_void_p),
+                  q.ctypes.data_as(C.c_void_p), qhi.ctypes.data_as(C.c_void_p))
+        return qlo[: self.s_nbv_xmin], q, qhi[: self.s_nbv_xmax]
+
+
+class SplineEvaluator:
+    """ddc::SplineEvaluator<..., LowerExtrapolationRule, UpperExtrapolationRule>."""
+
+    def __init__(self, bsplines: BSplines, lower_extrapolation: int = EXTRAP_NULL,
+                 upper_extrapolation: int = EXTRAP_NULL):
+        if bsplines.periodic:
+            lower_extrapolation = upper_extrapolation = EXTRAP_PERIODIC
+        self.bsplines = bsplines
+        h = C.c_void_p()
+        _lib.call("ddcb_evaluator_create", bsplines._h, int(lower_extrapolation), int(upper_extrapolation), C.byref(h))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.load().ddcb_evaluator_destroy(h)
+            self._h = None
+
+    def __call__(self, spline_eval, coords_eval, spline_coef, *, dim: int = 0, stream=None):
+        """SplineEvaluator::operator()(spline_eval, coords_eval, spline_coef)."""
+        out = _dev_f64(spline_eval, "spline_eval")
+        x = _dev_f64(coords_eval, "coords_eval")
+        c = _dev_f64(spline_coef, "spline_coef")
+        _lib.call("ddcb_eval", self._h, _ptr(out), lines_of(out, dim), _ptr(x), lines_of(x, dim), _ptr(c),
+                  lines_of(c, dim), _stream_handle(stream))
+        return out
+
+    def deriv(self, order: int, spline_eval, coords_eval, spline_coef, *, dim: int = 0, stream=None):
+        """SplineEvaluator::deriv(DiscreteElement<Deriv<X>>(order), spline_eval, coords_eval, spline_coef)."""
+        out = _dev_f64(spline_eval, "spline_eval")
+        x = _dev_f64(coords_eval, "coords_eval")
+        c = _dev_f64(spline_coef, "spline_coef")
+        _lib.call("ddcb_eval_deriv", self._h, int(order), _ptr(out), lines_of(out, dim), _ptr(x), lines_of(x, dim),
+                  _ptr(c), lines_of(c, dim), _stream_handle(stream))
+        return out
+
+    def integrate(self, integrals, spline_coef, *, dim: int = 0, stream=None):
+        """SplineEvaluator::integrate(integrals, spline_coef): integrals has the batch shape of spline_coef."""
+        out = _dev_f64(integrals, "integrals")
+        c = _dev_f64(spline_coef, "spline_coef")
+        lc = lines_of(c, dim)
+        assert out.numel() == lc.inner * lc.outer and out.is_contiguous()
+        _lib.call("ddcb_integrate", self._h, _ptr(out), lc.inner, _ptr(c), lc, _stream_handle(stream))
+        return out

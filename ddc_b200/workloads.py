@@ -1,0 +1,68 @@
+"""Seeded synthetic inputs of the five benchmark configurations (shared by tests and bench.py).
+
+Random numbers: splitmix64 streams turned into 53-bit uniforms; the seed of configuration c is
+0xDDC0 + c and every quantity draws from its own stream (stream id in the high bits).
+Arrays use the (row, line) layout with the batch contiguous: DDC's (x, batch) layout_right.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+
+
+def splitmix_uniform(seed: int, stream: int, n: int) -> np.ndarray:
+    """n uniforms in [0, 1) from the splitmix64 sequence of (seed, stream)."""
+    with np.errstate(over="ignore"):
+        base = np.uint64((seed + (stream << 40)) & 0xFFFFFFFFFFFFFFFF)
+        x = base + (np.arange(1, n + 1, dtype=np.uint64) * _GOLDEN)
+        z = x
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return (z >> np.uint64(11)).astype(np.float64) * (1.0 / (1 << 53))
+
+
+def cos_family(x, k, ph, order=0):
+    """d^order/dx^order cos(2 pi k x + ph) (the reference's CosineEvaluator, cosine_evaluator.hpp:78-81)."""
+    return (2 * np.pi * k) ** order * np.cos(np.pi / 2 * order + 2 * np.pi * k * x + ph)
+
+
+def config1(B: int = 1000, ncells: int = 1000, m: int = 1000):
+    """Periodic uniform cubic on [0,1): samples at the Greville points x_i = i/ncells, eval near grid points."""
+    seed = 0xDDC0 + 1
+    h = 1.0 / ncells
+    x = np.arange(ncells) * h
+    k = np.floor(splitmix_uniform(seed, 1, B) * 8).astype(np.int64) + 1
+    ph = splitmix_uniform(seed, 2, B) * 2 * np.pi
+    vals = cos_family(x[:, None], k[None, :], ph[None, :])
+    pts_idx = np.arange(m) % ncells
+    coords = (pts_idx * h)[:, None] + (splitmix_uniform(seed, 3, m * B).reshape(m, B) - 0.5) * h
+    coords = np.mod(coords, 1.0)
+    return dict(degree=3, ncells=ncells, x=x, k=k, ph=ph, vals=np.ascontiguousarray(vals),
+                coords=np.ascontiguousarray(coords))
+
+
+def config2_breaks(ncells: int = 1024):
+    seed = 0xDDC0 + 2
+    h = 1.0 / ncells
+    br = np.arange(ncells + 1) * h
+    br[1:-1] += (splitmix_uniform(seed, 1, ncells - 1) - 0.5) * 0.6 * h
+    br.sort()
+    br[0], br[-1] = 0.0, 1.0
+    return br
+
+
+def config2(B: int = 1 << 16, ncells: int = 1024, m: int = 1024, points=None):
+    """Non-uniform quintic, Hermite closures (derivative orders 1 and 2 per side), d/dx evaluation."""
+    seed = 0xDDC0 + 2
+    br = config2_breaks(ncells)
+    k = np.floor(splitmix_uniform(seed, 2, B) * 8).astype(np.int64) + 1
+    ph = splitmix_uniform(seed, 3, B) * 2 * np.pi
+    out = dict(degree=5, ncells=ncells, breaks=br, k=k, ph=ph)
+    if points is not None:
+        out["vals"] = np.ascontiguousarray(cos_family(points[:, None], k[None, :], ph[None, :]))
+        out["dlo"] = np.ascontiguousarray(np.stack([cos_family(0.0, k, ph, o) for o in (1, 2)]))
+        out["dhi"] = np.ascontiguousarray(np.stack([cos_family(1.0, k, ph, o) for o in (1, 2)]))
+    out["coords"] = np.ascontiguousarray(splitmix_uniform(seed, 4, m * B).reshape(m, B))
+    return out

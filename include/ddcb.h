@@ -1,0 +1,164 @@
+/* ddcb.h -- C-ABI of the B200 batched spline builder / evaluator.
+ *
+ * This is the drop-in boundary for DDC's batched spline hot path (CExA-project/ddc v0.15.1,
+ * src/ddc/kernels/splines/). Every entry point names the reference interface it replaces. The ABI
+ * carries plain pointers, sizes and strides only: device pointers for the batched data (the
+ * reference's ChunkSpans live in a Kokkos memory space), host pointers for mesh descriptions.
+ *
+ * Conventions
+ *  - Every function returns a ddcb_status; no C++ exception crosses the ABI. The text of the last
+ *    failure on the calling thread is returned by ddcb_last_error_message().
+ *  - Batched arrays are described by ddcb_lines: element (i, b) of line b is at
+ *        base[i*stride + (b / inner)*outer_stride + (b % inner)]
+ *    i.e. the dimension of interest has element stride `stride` and the batch dimensions are
+ *    flattened into (outer, inner) with the inner part contiguous. This covers every
+ *    layout_right dimension order of the reference's batched domains (interest dimension first,
+ *    middle or last, tests/splines/batched_spline_builder.cpp:393-515).
+ *  - Work is stream ordered on the ddcb_stream given (a cudaStream_t; NULL = legacy default).
+ *  - Plans (bases, builders, evaluators) are immutable after creation; calls on different streams
+ *    may run concurrently.
+ */
+#ifndef DDCB_H
+#define DDCB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* cudaStream_t without requiring the CUDA headers. */
+typedef struct CUstream_st* ddcb_stream;
+
+typedef enum ddcb_status {
+    DDCB_SUCCESS = 0,
+    DDCB_ERR_INVALID_ARGUMENT = 1, /* bad pointer, size, layout or enum */
+    DDCB_ERR_BAD_GRID = 2,         /* spline_builder.hpp:1244-1317 check_valid_grid failures */
+    DDCB_ERR_SINGULAR = 3,         /* a factorisation met a zero / non-positive pivot (LAPACK info != 0) */
+    DDCB_ERR_CUDA = 4,             /* a CUDA runtime call failed */
+    DDCB_ERR_UNSUPPORTED = 5,      /* valid request outside this implementation's limits */
+    DDCB_ERR_NOT_CONVERGED = 6,    /* iterative refinement did not reach its tolerance */
+    DDCB_ERR_DEVICE = 7            /* a kernel reported a failure through its status word */
+} ddcb_status;
+
+/* ddc::SplineBuilderClosure (spline_builder_closures.hpp:18-23). */
+typedef enum ddcb_closure {
+    DDCB_PERIODIC = 0,
+    DDCB_HERMITE = 1,
+    DDCB_HOMOGENEOUS_HERMITE = 2,
+    DDCB_GREVILLE = 3
+} ddcb_closure;
+
+/* The evaluator's extrapolation rules: PeriodicExtrapolationRule, NullExtrapolationRule,
+ * ConstantExtrapolationRule (periodic_/null_/constant_extrapolation_rule.hpp). */
+typedef enum ddcb_extrapolation {
+    DDCB_EXTRAP_PERIODIC = 0,
+    DDCB_EXTRAP_NULL = 1,
+    DDCB_EXTRAP_CONSTANT = 2
+} ddcb_extrapolation;
+
+/* Arithmetic of the batched solves. FP64 is the drop-in (the reference's SplineSolver::LAPACK
+ * arithmetic). FP32_REFINE solves in FP32 and refines with FP64 residuals; inputs and outputs stay
+ * FP64. */
+typedef enum ddcb_precision { DDCB_FP64 = 0, DDCB_FP32_REFINE = 1 } ddcb_precision;
+
+typedef struct ddcb_lines {
+    int64_t n;            /* extent along the dimension of interest */
+    int64_t stride;       /* element stride along the dimension of interest */
+    int64_t inner;        /* lines that are contiguous in memory (unit stride) */
+    int64_t outer;        /* groups of `inner` lines */
+    int64_t outer_stride; /* element stride between groups */
+} ddcb_lines;
+
+typedef struct ddcb_bsplines_t* ddcb_bsplines;
+typedef struct ddcb_builder_t* ddcb_builder;
+typedef struct ddcb_evaluator_t* ddcb_evaluator;
+
+typedef struct ddcb_bsplines_info {
+    int32_t degree, periodic, uniform;
+    int64_t ncells, nbasis, size; /* nbasis(), size() of bsplines_uniform.hpp:309-354 */
+    double rmin, rmax;
+} ddcb_bsplines_info;
+
+typedef struct ddcb_builder_options {
+    int32_t precision;     /* ddcb_precision */
+    int32_t refine_rounds; /* FP32_REFINE: refinement rounds (1..3) */
+    int32_t tile_lines;    /* 0 = automatic: lines per thread block */
+    int32_t chunks;        /* 0 = automatic: chunk threads per line */
+} ddcb_builder_options;
+
+typedef struct ddcb_builder_info {
+    int64_t nbasis, size, npoints;
+    int32_t nbe_lo, nbe_hi, nbv_lo, nbv_hi; /* s_nbe_xmin/xmax, s_nbv_xmin/xmax (spline_builder.hpp:166-191) */
+    int32_t offset;                         /* m_offset (spline_builder.hpp:201, 619-658) */
+    double dx;                              /* m_dx (spline_builder.hpp:233-234) */
+    int32_t border, kl, ku, pivoting, chunks, tile_lines; /* structure of the device solve */
+} ddcb_builder_info;
+
+/* ---- status ---------------------------------------------------------------------------- */
+const char* ddcb_status_string(ddcb_status s);
+const char* ddcb_last_error_message(void);
+
+/* ---- basis: UniformBSplines<CDim,D>::Impl(rmin, rmax, ncells) (bsplines_uniform.hpp:145-155)
+ *      and NonUniformBSplines<CDim,D>::Impl(breaks) (bsplines_non_uniform.hpp:414-457). ------- */
+ddcb_status ddcb_bsplines_create_uniform(int32_t degree, int32_t periodic, double rmin, double rmax,
+                                         int64_t ncells, ddcb_bsplines* out);
+ddcb_status ddcb_bsplines_create_non_uniform(int32_t degree, int32_t periodic, const double* breaks,
+                                             int64_t nbreaks, ddcb_bsplines* out);
+ddcb_status ddcb_bsplines_destroy(ddcb_bsplines b);
+ddcb_status ddcb_bsplines_get_info(ddcb_bsplines b, ddcb_bsplines_info* info);
+/* Knot coordinates (ddc::coordinate of the knot elements), `count` from index `first`. */
+ddcb_status ddcb_bsplines_knots(ddcb_bsplines b, int64_t first, int64_t count, double* out);
+/* GrevilleInterpolationPoints<BSplines, lo, hi>::get_sampling / get_domain
+ * (greville_interpolation_points.hpp:47-296): writes the interpolation points. */
+ddcb_status ddcb_greville_points(ddcb_bsplines b, ddcb_closure lo, ddcb_closure hi, double* points,
+                                 int64_t capacity, int64_t* npoints);
+/* integrals(execution_space, int_vals) (integrals.hpp:165-177), host output of size() entries. */
+ddcb_status ddcb_bsplines_integrals(ddcb_bsplines b, double* out);
+
+/* ---- builder: SplineBuilder<..., SplineSolver> constructor (spline_builder.hpp:227-260):
+ *      check_valid_grid, compute_offset, allocate_matrix / build_matrix_system / setup_solver,
+ *      with the device plan created on the current CUDA device. ------------------------------ */
+ddcb_status ddcb_builder_create(ddcb_bsplines basis, const double* interp_points, int64_t npoints,
+                                ddcb_closure lo, ddcb_closure hi, const ddcb_builder_options* options,
+                                ddcb_builder* out);
+ddcb_status ddcb_builder_destroy(ddcb_builder b);
+ddcb_status ddcb_builder_get_info(ddcb_builder b, ddcb_builder_info* info);
+/* SplineBuilder::operator()(spline, vals, derivs_xmin, derivs_xmax) (spline_builder.hpp:538-557,
+ * 896-1101). derivs_* are ignored (may be NULL) unless the closure is HERMITE; their layout's n is
+ * s_nbv (derivative orders odd..odd+nbv-1, unscaled). */
+ddcb_status ddcb_build(ddcb_builder b, double* coefs, ddcb_lines coefs_layout, const double* vals,
+                       ddcb_lines vals_layout, const double* derivs_lo, ddcb_lines derivs_lo_layout,
+                       const double* derivs_hi, ddcb_lines derivs_hi_layout, ddcb_stream stream);
+/* SplinesLinearProblem::solve(MultiRHS b, bool transpose) (splines_linear_problem.hpp:80-92):
+ * in-place solve of A x = b (or A^T x = b) for nrhs columns of a (nbasis x nrhs) row-major device
+ * array with leading dimension ld (>= nrhs). */
+ddcb_status ddcb_solve_multirhs(ddcb_builder b, double* rhs, int64_t ld, int64_t nrhs, int32_t transpose,
+                                ddcb_stream stream);
+/* SplineBuilder::quadrature_coefficients() (spline_builder.hpp:1103-1234), host outputs of
+ * nbv_lo, nbasis - nbv_lo - nbv_hi and nbv_hi entries; the Hermite parts are scaled by dx^k. */
+ddcb_status ddcb_quadrature_coefficients(ddcb_builder b, double* q_derivs_lo, double* q_vals, double* q_derivs_hi);
+
+/* ---- evaluator: SplineEvaluator<..., LowerExtrapolationRule, UpperExtrapolationRule>
+ *      (spline_evaluator.hpp:160-186). ------------------------------------------------------- */
+ddcb_status ddcb_evaluator_create(ddcb_bsplines basis, ddcb_extrapolation lo, ddcb_extrapolation hi,
+                                  ddcb_evaluator* out);
+ddcb_status ddcb_evaluator_destroy(ddcb_evaluator e);
+/* SplineEvaluator::operator()(spline_eval, coords_eval, spline_coef) (spline_evaluator.hpp:257-294). */
+ddcb_status ddcb_eval(ddcb_evaluator e, double* out, ddcb_lines out_layout, const double* coords,
+                      ddcb_lines coords_layout, const double* coefs, ddcb_lines coefs_layout, ddcb_stream stream);
+/* SplineEvaluator::deriv(deriv_order, spline_eval, coords_eval, spline_coef)
+ * (spline_evaluator.hpp:388-430); order in 1..degree, no boundary handling (eval_no_bc). */
+ddcb_status ddcb_eval_deriv(ddcb_evaluator e, int32_t order, double* out, ddcb_lines out_layout,
+                            const double* coords, ddcb_lines coords_layout, const double* coefs,
+                            ddcb_lines coefs_layout, ddcb_stream stream);
+/* SplineEvaluator::integrate(integrals, spline_coef) (spline_evaluator.hpp:493-526): one value per
+ * line, out[(b / inner)*out_outer_stride + b % inner] with the coefficient layout's batch shape. */
+ddcb_status ddcb_integrate(ddcb_evaluator e, double* out, int64_t out_outer_stride, const double* coefs,
+                           ddcb_lines coefs_layout, ddcb_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DDCB_H */
