@@ -83,6 +83,8 @@ SIGNATURES = {
     "ddcb_eval": [_vp, _vp, Lines, _vp, Lines, _vp, Lines, _vp],
     "ddcb_eval_deriv": [_vp, C.c_int32, _vp, Lines, _vp, Lines, _vp, Lines, _vp],
     "ddcb_integrate": [_vp, _vp, C.c_int64, _vp, Lines, _vp],
+    "ddcb_build_eval": [_vp, _vp, C.c_int32, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines,
+                        C.POINTER(C.c_int32), _vp],
 }
 
 _lib = None

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libddcb.so")
-SOURCES = ["api.cu", "plan.cpp", "build_kernels.cu", "eval_kernels.cu"]
+SOURCES = ["api.cu", "plan.cpp", "build_kernels.cu", "eval_kernels.cu", "fused_kernels.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -35,14 +35,36 @@ def needs_build() -> bool:
 
 
 def build(verbose: bool = False, force: bool = False) -> str:
+    """Compile every source to an object in parallel, then link libddcb.so."""
     if not force and not needs_build():
         return LIB
-    cmd = [nvcc(), "-std=c++17", "-O3", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-shared",
-           "-ccbin", "g++", "--expt-relaxed-constexpr", "-o", LIB, *sources()]
+    from concurrent.futures import ThreadPoolExecutor
+
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    common = [nvcc(), "-std=c++17", "-O3", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-ccbin", "g++",
+              "--expt-relaxed-constexpr"]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd), flush=True)
-    subprocess.run(cmd, check=True)
+        common.append("-Xptxas=-v")
+
+    def compile_one(src):
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        cmd = [*common, "-c", "-o", obj, src]
+        if src.endswith(".cpp"):
+            cmd = [*common, "-x", "cu", "-c", "-o", obj, src]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        return src, obj, r
+
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        results = list(ex.map(compile_one, sources()))
+    for src, obj, r in results:
+        if verbose or r.returncode:
+            sys.stdout.write(r.stdout)
+            sys.stderr.write(r.stderr)
+        if r.returncode:
+            raise subprocess.CalledProcessError(r.returncode, src)
+    link = [nvcc(), *ARCH, "-shared", "-o", LIB, *[o for _, o, _ in results]]
+    subprocess.run(link, check=True)
     return LIB
 
 

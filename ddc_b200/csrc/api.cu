@@ -293,35 +293,76 @@ ddcb_status ddcb_builder_get_info(ddcb_builder h, ddcb_builder_info* info)
     });
 }
 
+// Validates a build call; returns false for an empty batch. Clears derivative pointers the
+// closures do not read.
+static bool check_build(ddcb_builder h, double* coefs, ddcb_lines lc, const double* vals, ddcb_lines lv,
+                        const double*& dlo, ddcb_lines llo, const double*& dhi, ddcb_lines lhi)
+{
+    require(h != nullptr, "builder is NULL");
+    ddcb::Builder const& b = *h->b;
+    check_lines(lv, int64_t(b.points.size()), "vals");
+    check_lines(lc, b.basis.size(), "coefs");
+    same_batch(lv, lc, "coefs/vals");
+    if (lv.inner * lv.outer == 0) return false; // empty batch: nothing to do (spline_builder.hpp:929-931)
+    require(vals && coefs, "vals/coefs pointer is NULL");
+    if (b.lo == DDCB_HERMITE && b.nbv_lo > 0) {
+        require(dlo != nullptr, "derivs_lo is required by the lower HERMITE closure");
+        check_lines(llo, b.nbv_lo, "derivs_lo");
+        same_batch(llo, lv, "derivs_lo/vals");
+    } else {
+        dlo = nullptr;
+    }
+    if (b.hi == DDCB_HERMITE && b.nbv_hi > 0) {
+        require(dhi != nullptr, "derivs_hi is required by the upper HERMITE closure");
+        check_lines(lhi, b.nbv_hi, "derivs_hi");
+        same_batch(lhi, lv, "derivs_hi/vals");
+    } else {
+        dhi = nullptr;
+    }
+    int dev = 0;
+    DDCB_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev != b.device) throw ddcb::Error(DDCB_ERR_INVALID_ARGUMENT, "the builder was created for another device");
+    return true;
+}
+
+ddcb_status ddcb_build_eval(ddcb_builder h, ddcb_evaluator he, int32_t order, double* coefs, ddcb_lines lc,
+                            const double* vals, ddcb_lines lv, const double* dlo, ddcb_lines llo, const double* dhi,
+                            ddcb_lines lhi, const double* coords, ddcb_lines lx, double* out, ddcb_lines lo,
+                            int32_t* fused, ddcb_stream stream)
+{
+    return guarded([&] {
+        if (fused) *fused = 0;
+        require(he != nullptr, "evaluator is NULL");
+        ddcb::Evaluator const& e = *he->e;
+        require(order >= 0 && order <= e.basis.desc.degree, "derivative order must be in 0..degree");
+        if (!check_build(h, coefs, lc, vals, lv, dlo, llo, dhi, lhi)) return;
+        ddcb::Builder const& b = *h->b;
+        require(e.basis.desc.degree == b.basis.desc.degree && e.basis.desc.ncells == b.basis.desc.ncells
+                    && e.basis.desc.uniform == b.basis.desc.uniform && e.basis.desc.periodic == b.basis.desc.periodic,
+                "builder and evaluator use different bases");
+        check_lines(lx, lx.n, "coords");
+        check_lines(lo, lx.n, "out");
+        same_batch(lx, lo, "coords/out");
+        same_batch(lx, lv, "coords/vals");
+        if (lx.n == 0) {
+            ddcb::launch_build(b, coefs, ddcb::to_lines(lc), vals, ddcb::to_lines(lv), dlo, ddcb::to_lines(llo), dhi,
+                               ddcb::to_lines(lhi), reinterpret_cast<cudaStream_t>(stream));
+            return;
+        }
+        require(coords && out, "coords/out pointer is NULL");
+        bool const f = ddcb::launch_build_eval(b, e, order, coefs, ddcb::to_lines(lc), vals, ddcb::to_lines(lv), dlo,
+                                               ddcb::to_lines(llo), dhi, ddcb::to_lines(lhi), coords, ddcb::to_lines(lx),
+                                               out, ddcb::to_lines(lo), reinterpret_cast<cudaStream_t>(stream));
+        if (fused) *fused = f ? 1 : 0;
+    });
+}
+
 ddcb_status ddcb_build(ddcb_builder h, double* coefs, ddcb_lines lc, const double* vals, ddcb_lines lv,
                        const double* dlo, ddcb_lines llo, const double* dhi, ddcb_lines lhi, ddcb_stream stream)
 {
     return guarded([&] {
-        require(h != nullptr, "builder is NULL");
+        if (!check_build(h, coefs, lc, vals, lv, dlo, llo, dhi, lhi)) return;
         ddcb::Builder const& b = *h->b;
-        check_lines(lv, int64_t(b.points.size()), "vals");
-        check_lines(lc, b.basis.size(), "coefs");
-        same_batch(lv, lc, "coefs/vals");
-        int64_t const nl = lv.inner * lv.outer;
-        if (nl == 0) return; // empty batch: nothing to do (spline_builder.hpp:929-931)
-        require(vals && coefs, "vals/coefs pointer is NULL");
-        if (b.lo == DDCB_HERMITE && b.nbv_lo > 0) {
-            require(dlo != nullptr, "derivs_lo is required by the lower HERMITE closure");
-            check_lines(llo, b.nbv_lo, "derivs_lo");
-            same_batch(llo, lv, "derivs_lo/vals");
-        } else {
-            dlo = nullptr;
-        }
-        if (b.hi == DDCB_HERMITE && b.nbv_hi > 0) {
-            require(dhi != nullptr, "derivs_hi is required by the upper HERMITE closure");
-            check_lines(lhi, b.nbv_hi, "derivs_hi");
-            same_batch(lhi, lv, "derivs_hi/vals");
-        } else {
-            dhi = nullptr;
-        }
-        int dev = 0;
-        DDCB_CUDA_CHECK(cudaGetDevice(&dev));
-        if (dev != b.device) throw ddcb::Error(DDCB_ERR_INVALID_ARGUMENT, "the builder was created for another device");
         ddcb::launch_build(b, coefs, ddcb::to_lines(lc), vals, ddcb::to_lines(lv), dlo, ddcb::to_lines(llo), dhi,
                            ddcb::to_lines(lhi), reinterpret_cast<cudaStream_t>(stream));
     });

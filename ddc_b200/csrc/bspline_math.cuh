@@ -11,6 +11,7 @@
 // Keeping the same operation order keeps results within a few ulps of the reference's.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 
 #if defined(__CUDACC__)

@@ -152,6 +152,10 @@ void builder_quadrature(Builder const& b, double* qlo, double* q, double* qhi);
 void launch_build(Builder const& b, double* coefs, Lines const& lc, double const* vals, Lines const& lv,
                   double const* dlo, Lines const& llo, double const* dhi, Lines const& lhi, cudaStream_t s);
 void launch_solve_multirhs(Builder const& b, double* rhs, long ld, long nrhs, bool transpose, cudaStream_t s);
+// Builder then evaluator on the same lines; returns true when the single fused kernel ran.
+bool launch_build_eval(Builder const& b, Evaluator const& e, int order, double* coefs, Lines const& lc,
+                       double const* vals, Lines const& lv, double const* dlo, Lines const& llo, double const* dhi,
+                       Lines const& lhi, double const* coords, Lines const& lx, double* out, Lines const& lo, cudaStream_t s);
 
 // eval_kernels.cu
 void launch_eval(Evaluator const& e, int order, double* out, Lines const& lo, double const* coords, Lines const& lx,

@@ -18,6 +18,31 @@ struct EvalBasis
 
 #if defined(__CUDACC__)
 
+// Coefficient of B-spline b of one line: C[b*cs] (coefficients stored in basis order).
+struct CoefDirect
+{
+    const double* C;
+    int cs;
+    __device__ __forceinline__ double operator()(int b) const { return C[b * cs]; }
+};
+
+// Coefficients still in the builder's column order inside its tile: B-spline b lives in column
+// (b mod n) - offset (mod n) (spline_builder.hpp:1061-1100).
+struct CoefRotated
+{
+    const double* C;
+    int cs;
+    int n;
+    int offset;
+    __device__ __forceinline__ double operator()(int b) const
+    {
+        int r = (b >= n ? b - n : b) - offset;
+        r += (r < 0) ? n : 0;
+        r -= (r >= n) ? n : 0;
+        return C[r * cs];
+    }
+};
+
 // Cell of x as a knot index (the cell [t_c, t_c+1) with t_c <= x < t_c+1), with the end rules of
 // bsplines_non_uniform.hpp:666-695. A bucket table gives a starting cell; short walks finish it,
 // so the result equals the bisection's for any mesh.
@@ -38,8 +63,8 @@ __device__ __forceinline__ int nonuniform_locate(EvalBasis const& eb, double x)
 
 // s(x) without boundary handling (spline_evaluator.hpp:556-605). C[i*cs] is the coefficient of
 // B-spline i.
-template <int D, bool UNI>
-__device__ __forceinline__ double eval_value_no_bc(EvalBasis const& eb, double x, const double* C, int cs)
+template <int D, bool UNI, class Acc>
+__device__ __forceinline__ double eval_value_no_bc(EvalBasis const& eb, double x, Acc const& C)
 {
     double v[D + 1];
     int jmin;
@@ -54,15 +79,15 @@ __device__ __forceinline__ double eval_value_no_bc(EvalBasis const& eb, double x
     }
     double y = 0.0;
 #pragma unroll
-    for (int i = 0; i < D + 1; ++i) y = fma(C[(jmin + i) * cs], v[i], y);
+    for (int i = 0; i < D + 1; ++i) y = fma(C(jmin + i), v[i], y);
     return y;
 }
 
 // s(x) with the periodic wrap or the extrapolation rules (spline_evaluator.hpp:529-554,
 // null_extrapolation_rule.hpp:14-26, constant_extrapolation_rule.hpp:27-52 evaluated at the
 // domain end).
-template <int D, bool UNI>
-__device__ __forceinline__ double eval_value_bc(EvalBasis const& eb, int ex_lo, int ex_hi, double x, const double* C, int cs)
+template <int D, bool UNI, class Acc>
+__device__ __forceinline__ double eval_value_bc(EvalBasis const& eb, int ex_lo, int ex_hi, double x, Acc const& C)
 {
     if (eb.b.periodic) {
         x = periodic_wrap(eb.b, x);
@@ -75,13 +100,13 @@ __device__ __forceinline__ double eval_value_bc(EvalBasis const& eb, int ex_lo, 
             x = eb.b.rmax;
         }
     }
-    return eval_value_no_bc<D, UNI>(eb, x, C, cs);
+    return eval_value_no_bc<D, UNI>(eb, x, C);
 }
 
 // d^ORDER s / dx^ORDER at x (spline_evaluator.hpp:388-430, no boundary handling): ORDER rounds of
 // divided differences of the d+1 coefficients of the cell, then the degree-(D-ORDER) basis.
-template <int D, int ORDER, bool UNI>
-__device__ __forceinline__ double eval_deriv_no_bc(EvalBasis const& eb, double x, const double* C, int cs)
+template <int D, int ORDER, bool UNI, class Acc>
+__device__ __forceinline__ double eval_deriv_no_bc(EvalBasis const& eb, double x, Acc const& C)
 {
     constexpr int P = D - ORDER;
     double cc[D + 1];
@@ -97,7 +122,7 @@ __device__ __forceinline__ double eval_deriv_no_bc(EvalBasis const& eb, double x
         jmin = ck - D;
     }
 #pragma unroll
-    for (int i = 0; i < D + 1; ++i) cc[i] = C[(jmin + i) * cs];
+    for (int i = 0; i < D + 1; ++i) cc[i] = C(jmin + i);
 #pragma unroll
     for (int k = 1; k <= ORDER; ++k) {
 #pragma unroll
@@ -114,6 +139,14 @@ __device__ __forceinline__ double eval_deriv_no_bc(EvalBasis const& eb, double x
 #pragma unroll
     for (int r = 0; r < P + 1; ++r) y = fma(cc[ORDER + r], v[r], y);
     return y;
+}
+
+// Value (ORDER 0, with boundary handling) or ORDER-th derivative (no boundary handling).
+template <int D, int ORDER, bool UNI, class Acc>
+__device__ __forceinline__ double eval_point(EvalBasis const& eb, int ex_lo, int ex_hi, double x, Acc const& C)
+{
+    if constexpr (ORDER == 0) return eval_value_bc<D, UNI>(eb, ex_lo, ex_hi, x, C);
+    else return eval_deriv_no_bc<D, ORDER, UNI>(eb, x, C);
 }
 
 #endif // __CUDACC__

@@ -36,6 +36,12 @@ __device__ __forceinline__ int64_t line_offset(Lines const& L, int64_t b)
     return (b / L.inner) * L.outer_stride + (b % L.inner);
 }
 
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src)
+{
+    unsigned const s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+
 template <int D, int TLE, int ORDER, bool UNI>
 __global__ void __launch_bounds__(256) eval_kernel(const __grid_constant__ EvalArgs a)
 {
@@ -50,10 +56,11 @@ __global__ void __launch_bounds__(256) eval_kernel(const __grid_constant__ EvalA
     bool const live = line < a.nlines;
     if (live) {
         int64_t const oc = line_offset(a.lc, line);
-        for (int r = c; r < a.size; r += nct) C[r * TLE + l] = a.coefs[r * a.lc.stride + oc];
+        for (int r = c; r < a.size; r += nct) cp_async8(C + r * TLE + l, a.coefs + r * a.lc.stride + oc);
     }
     if (!UNI)
-        for (int i = tid; i < a.eb.nk; i += blockDim.x) K[i] = a.eb.b.knots[i];
+        for (int i = tid; i < a.eb.nk; i += blockDim.x) cp_async8(K + i, a.eb.b.knots + i);
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
     if (!live) return;
     EvalBasis eb = a.eb;
@@ -61,12 +68,22 @@ __global__ void __launch_bounds__(256) eval_kernel(const __grid_constant__ EvalA
     int64_t const ox = line_offset(a.lx, line);
     int64_t const oo = line_offset(a.lo, line);
     int64_t const m = a.lx.n;
-    for (int64_t p = c; p < m; p += nct) {
-        double const x = a.coords[p * a.lx.stride + ox];
-        double y;
-        if (ORDER == 0) y = eval_value_bc<D, UNI>(eb, a.ex_lo, a.ex_hi, x, C + l, TLE);
-        else y = eval_deriv_no_bc<D, ORDER, UNI>(eb, x, C + l, TLE);
-        a.out[p * a.lo.stride + oo] = y;
+    CoefDirect const acc {C + l, TLE};
+    const double* __restrict__ coords = a.coords;
+    double* __restrict__ out = a.out;
+    constexpr int U = 4; // points in flight per thread
+    for (int64_t p0 = c; p0 < m; p0 += (int64_t)U * nct) {
+        double xs[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            int64_t const p = p0 + (int64_t)u * nct;
+            xs[u] = p < m ? coords[p * a.lx.stride + ox] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            int64_t const p = p0 + (int64_t)u * nct;
+            if (p < m) out[p * a.lo.stride + oo] = eval_point<D, ORDER, UNI>(eb, a.ex_lo, a.ex_hi, xs[u], acc);
+        }
     }
 }
 

@@ -1,0 +1,127 @@
+// fused_kernels.cu -- build + evaluate in one kernel (the semi-Lagrangian step of
+// examples/characteristics_advection.cpp:251-259: SplineBuilder::operator() then
+// SplineEvaluator::operator() / deriv on the same lines).
+//
+// The tile solved in shared memory by solve_tile is stored as the coefficient output and then
+// evaluated in place: the coefficients are written once and never read back from HBM. Kernels
+// exist for the band shapes and tile width the configurations use; any other combination runs the
+// builder and the evaluator kernels one after the other (same results).
+#include "build_device.cuh"
+#include "eval_device.cuh"
+
+namespace ddcb {
+
+namespace {
+
+struct FusedEval
+{
+    EvalBasis eb;
+    int ex_lo, ex_hi;
+    const double* coords;
+    Lines lx;
+    double* out;
+    Lines lo;
+};
+
+template <int TL, int KL, int KU, int D, int ORDER, bool UNI>
+__global__ void __launch_bounds__(1024) build_eval_kernel(const __grid_constant__ BuildArgs args,
+                                                          const __grid_constant__ FusedEval fe)
+{
+    extern __shared__ double smem[];
+    double* K = smem + tile_doubles(args.t, TL, KL, KU); // knots (non-uniform)
+    if (!UNI)
+        for (int i = threadIdx.x; i < fe.eb.nk; i += blockDim.x) K[i] = fe.eb.b.knots[i];
+    solve_tile<TL, KL, KU>(args, smem);
+    store_tile<TL>(args, smem);
+    int const tid = threadIdx.x;
+    int const l = tid % TL;
+    int const c = tid / TL;
+    int const nct = args.nct;
+    int64_t const line = (int64_t)blockIdx.x * TL + l;
+    if (line >= args.nlines) return;
+    EvalBasis eb = fe.eb;
+    if (!UNI) eb.b.knots = K;
+    int64_t const ox = line_offset(fe.lx, line);
+    int64_t const oo = line_offset(fe.lo, line);
+    int64_t const m = fe.lx.n;
+    CoefRotated const acc {smem + l, TL, args.t.n, args.r.periodic ? args.r.offset : 0};
+    const double* __restrict__ coords = fe.coords;
+    double* __restrict__ out = fe.out;
+    constexpr int U = 4;
+    for (int64_t p0 = c; p0 < m; p0 += (int64_t)U * nct) {
+        double xs[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            int64_t const p = p0 + (int64_t)u * nct;
+            xs[u] = p < m ? coords[p * fe.lx.stride + ox] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            int64_t const p = p0 + (int64_t)u * nct;
+            if (p < m) out[p * fe.lo.stride + oo] = eval_point<D, ORDER, UNI>(eb, fe.ex_lo, fe.ex_hi, xs[u], acc);
+        }
+    }
+}
+
+template <int KL, int KU, int D, int ORDER, bool UNI>
+bool launch5(BuildArgs const& args, FusedEval const& fe, cudaStream_t s)
+{
+    constexpr int TL = 8;
+    size_t const sm = sizeof(double) * (tile_doubles(args.t, TL, KL, KU) + (UNI ? 0 : (size_t)fe.eb.nk));
+    int dev = 0, optin = 0;
+    DDCB_CUDA_CHECK(cudaGetDevice(&dev));
+    DDCB_CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (sm > size_t(optin)) return false;
+    auto kern = build_eval_kernel<TL, KL, KU, D, ORDER, UNI>;
+    if (sm > 48 * 1024) DDCB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    int64_t const grid = (args.nlines + TL - 1) / TL;
+    kern<<<dim3((unsigned)grid), dim3(TL * args.nct), sm, s>>>(args, fe);
+    DDCB_CUDA_CHECK(cudaGetLastError());
+    return true;
+}
+
+template <int KL, int KU, int D>
+bool launch_ord(BuildArgs const& args, FusedEval const& fe, int order, bool uni, cudaStream_t s)
+{
+    if (order == 0) return uni ? launch5<KL, KU, D, 0, true>(args, fe, s) : launch5<KL, KU, D, 0, false>(args, fe, s);
+    if (order == 1) return uni ? launch5<KL, KU, D, 1, true>(args, fe, s) : launch5<KL, KU, D, 1, false>(args, fe, s);
+    return false;
+}
+
+template <int KL, int KU>
+bool launch_deg(BuildArgs const& args, FusedEval const& fe, int order, cudaStream_t s)
+{
+    bool const uni = fe.eb.b.uniform != 0;
+    switch (fe.eb.b.degree) {
+    case 1: return launch_ord<KL, KU, 1>(args, fe, order, uni, s);
+    case 2: return launch_ord<KL, KU, 2>(args, fe, order, uni, s);
+    case 3: return launch_ord<KL, KU, 3>(args, fe, order, uni, s);
+    case 4: return launch_ord<KL, KU, 4>(args, fe, order, uni, s);
+    case 5: return launch_ord<KL, KU, 5>(args, fe, order, uni, s);
+    default: return false;
+    }
+}
+
+} // namespace
+
+// Returns false when no fused kernel covers this combination (the caller then runs the two
+// kernels back to back).
+bool launch_build_eval_fused(BuildArgs const& args, Evaluator const& e, int order, double* out, Lines const& lo,
+                             double const* coords, Lines const& lx, cudaStream_t s)
+{
+    FusedEval fe {};
+    fe.eb = e.eb;
+    fe.ex_lo = e.ex_lo;
+    fe.ex_hi = e.ex_hi;
+    fe.coords = coords;
+    fe.lx = lx;
+    fe.out = out;
+    fe.lo = lo;
+    int const kl = args.t.kl, ku = args.t.ku;
+    if (kl == 1 && ku == 1) return launch_deg<1, 1>(args, fe, order, s);
+    if (kl == 2 && ku == 2) return launch_deg<2, 2>(args, fe, order, s);
+    if (kl == 4 && ku == 4) return launch_deg<4, 4>(args, fe, order, s);
+    return false;
+}
+
+} // namespace ddcb

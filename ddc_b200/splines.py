@@ -209,6 +209,25 @@ class SplineBuilder:
                   _stream_handle(stream))
         return spline
 
+    def build_and_evaluate(self, evaluator: "SplineEvaluator", spline, vals, coords_eval, spline_eval, derivs_xmin=None,
+                           derivs_xmax=None, *, order: int = 0, dim: int = 0, stream=None) -> bool:
+        """operator()(spline, vals, ...) then evaluator(spline_eval, coords_eval, spline) (order 0) or
+        evaluator.deriv(order, ...) on the same lines, fused into one kernel when one exists.
+        Returns True when the fused kernel ran."""
+        spline = _dev_f64(spline, "spline")
+        vals = _dev_f64(vals, "vals")
+        dlo = _dev_f64(derivs_xmin, "derivs_xmin")
+        dhi = _dev_f64(derivs_xmax, "derivs_xmax")
+        x = _dev_f64(coords_eval, "coords_eval")
+        out = _dev_f64(spline_eval, "spline_eval")
+        llo = lines_of(dlo, dim) if dlo is not None else Lines(0, 1, 0, 0, 0)
+        lhi = lines_of(dhi, dim) if dhi is not None else Lines(0, 1, 0, 0, 0)
+        fused = C.c_int32(0)
+        _lib.call("ddcb_build_eval", self._h, evaluator._h, int(order), _ptr(spline), lines_of(spline, dim), _ptr(vals),
+                  lines_of(vals, dim), _ptr(dlo), llo, _ptr(dhi), lhi, _ptr(x), lines_of(x, dim), _ptr(out),
+                  lines_of(out, dim), C.byref(fused), _stream_handle(stream))
+        return bool(fused.value)
+
     def solve(self, rhs, transpose: bool = False, stream=None):
         """In-place SplinesLinearProblem::solve on a (nbasis, nrhs) CUDA float64 matrix."""
         rhs = _dev_f64(rhs, "rhs")

@@ -157,6 +157,16 @@ ddcb_status ddcb_eval_deriv(ddcb_evaluator e, int32_t order, double* out, ddcb_l
 ddcb_status ddcb_integrate(ddcb_evaluator e, double* out, int64_t out_outer_stride, const double* coefs,
                            ddcb_lines coefs_layout, ddcb_stream stream);
 
+/* ---- fused step: SplineBuilder::operator() followed by SplineEvaluator::operator() (order 0)
+ *      or SplineEvaluator::deriv (order >= 1) on the same lines -- the semi-Lagrangian step of
+ *      examples/characteristics_advection.cpp:251-259. Writes both the coefficients and the
+ *      evaluated values; *fused (may be NULL) tells whether one kernel did both. ---------------- */
+ddcb_status ddcb_build_eval(ddcb_builder b, ddcb_evaluator e, int32_t order, double* coefs, ddcb_lines coefs_layout,
+                            const double* vals, ddcb_lines vals_layout, const double* derivs_lo,
+                            ddcb_lines derivs_lo_layout, const double* derivs_hi, ddcb_lines derivs_hi_layout,
+                            const double* coords, ddcb_lines coords_layout, double* out, ddcb_lines out_layout,
+                            int32_t* fused, ddcb_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

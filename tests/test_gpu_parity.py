@@ -189,3 +189,44 @@ def test_solve_multirhs_inverse(D, oracle_mod, degree, uniform, periodic, transp
     Xn = X.cpu().numpy()
     I = A @ Xn if not transpose else A.T @ Xn
     np.testing.assert_allclose(I, np.eye(n), atol=1e-10)
+
+
+@pytest.mark.parametrize("case", ["c1", "c2", "np_cubic_greville", "per_quartic_nonuniform"])
+def test_fused_build_eval_matches_two_calls(D, oracle_mod, case):
+    """ddcb_build_eval gives the same coefficients and values as ddcb_build + ddcb_eval(_deriv)."""
+    from ddc_b200 import workloads
+
+    O = oracle_mod
+    rng = np.random.default_rng(11)
+    if case == "c1":
+        bs, lo, order, B = D.UniformBSplines(3, True, 0.0, 1.0, 1000), 0, 0, 203
+    elif case == "c2":
+        bs, lo, order, B = D.NonUniformBSplines(5, False, workloads.config2_breaks()), 1, 1, 77
+    elif case == "np_cubic_greville":
+        bs, lo, order, B = D.UniformBSplines(3, False, 0.0, 2.0, 300), 3, 0, 64
+    else:
+        br = np.linspace(0.0, 1.0, 101)
+        br[1:-1] += rng.uniform(-0.003, 0.003, 99)
+        bs, lo, order, B = D.NonUniformBSplines(4, True, br), 0, 1, 50
+    pts = D.greville_points(bs, lo, lo)
+    builder = D.SplineBuilder(bs, pts, lo, lo)
+    ev = D.SplineEvaluator(bs)
+    vals = cuda(rng.standard_normal((pts.size, B)))
+    nd = builder.s_nbv_xmin
+    dlo = cuda(rng.standard_normal((nd, B))) if lo == 1 else None
+    dhi = cuda(rng.standard_normal((nd, B))) if lo == 1 else None
+    x = cuda(rng.uniform(bs.rmin, bs.rmax, (333, B)))
+    c1 = torch.zeros((bs.size, B), dtype=torch.float64, device="cuda")
+    o1 = torch.zeros((333, B), dtype=torch.float64, device="cuda")
+    fused = builder.build_and_evaluate(ev, c1, vals, x, o1, dlo, dhi, order=order)
+    c2 = torch.zeros_like(c1)
+    o2 = torch.zeros_like(o1)
+    builder(c2, vals, dlo, dhi)
+    if order == 0:
+        ev(o2, x, c2)
+    else:
+        ev.deriv(order, o2, x, c2)
+    assert torch.equal(c1, c2)
+    assert relerr(o1.cpu().numpy(), o2.cpu().numpy()) <= 1e-14
+    if case in ("c1", "c2"):
+        assert fused
