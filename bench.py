@@ -45,6 +45,8 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=0, help="steps of the host-buffer (e2e) timing; 0 = --steps")
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU time of the baseline sample")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--tile-lines", type=int, default=0, help="builder tile width (0 = plan default)")
+    p.add_argument("--chunks", type=int, default=0, help="builder chunks per line (0 = plan default)")
     return p.parse_args()
 
 
@@ -201,7 +203,8 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     lines, m = args.lines, 1024
     bs, pts, br = workload_plan(D, lines)
-    builder = D.SplineBuilder(bs, pts, D.SplineBuilderClosure.HERMITE, D.SplineBuilderClosure.HERMITE)
+    builder = D.SplineBuilder(bs, pts, D.SplineBuilderClosure.HERMITE, D.SplineBuilderClosure.HERMITE,
+                              tile_lines=args.tile_lines, chunks=args.chunks)
     ev = D.SplineEvaluator(bs)
     w = make_inputs(pts, lines, m)
     dev = torch.device("cuda", local)

@@ -10,7 +10,7 @@
 // carry with a transfer matrix fixed by the factors (precomputed on the host), so each sweep runs
 // in three phases:
 //   A: every chunk sweeps with a zero incoming carry and records its outgoing carry;
-//   B: one thread per line chains the carries through the transfer matrices;
+//   B: a log-depth scan over the chunks chains the carries through products of transfer matrices;
 //   C: every chunk sweeps again from its true carry and writes its rows.
 // Periodic systems add a border of k rows/cols (Schur complement; the 2x2 block solve of
 // splines_linear_problem_2x2_blocks.cpp:274-298) applied in shared memory.
@@ -105,6 +105,45 @@ __device__ __forceinline__ void bwd_sweep(SolveTables const& t, double* T, int T
     }
 }
 
+// Log-depth (Kogge-Stone) scan of the chunk carries. On entry carry[c] holds chunk c's outgoing
+// carry for a zero incoming carry; on exit it holds the true outgoing carry. Forward: chunk c's
+// carry flows into c+1, out(c) = Phi_c out(c-1) + hat(c); step k adds P(k,c) y(c-2^k). Backward:
+// the carry flows from c+1 into c with Q(k,c) y(c+2^k). Every thread of the block takes part in the
+// barriers; threads of chunk c < NC do the arithmetic.
+template <int K, int KC, int TL, bool FWD>
+__device__ __forceinline__ void carry_scan(const double* __restrict__ P, double* carry, int nscan, int NC, int c, int l)
+{
+    double y[K];
+    bool const act = c < NC;
+    if (act) {
+#pragma unroll
+        for (int q = 0; q < K; ++q) y[q] = carry[(c * KC + q) * TL + l];
+    }
+    for (int k = 0; k < nscan; ++k) {
+        int const nb = FWD ? c - (1 << k) : c + (1 << k);
+        bool const has = act && (FWD ? nb >= 0 : nb < NC);
+        double v[K];
+        if (has) {
+#pragma unroll
+            for (int q = 0; q < K; ++q) v[q] = carry[(nb * KC + q) * TL + l];
+        }
+        __syncthreads();
+        if (has) {
+            double const* M = P + ((size_t)k * NC + c) * K * K;
+#pragma unroll
+            for (int r = 0; r < K; ++r) {
+                double s = y[r];
+#pragma unroll
+                for (int q = 0; q < K; ++q) s = fma(__ldg(M + r * K + q), v[q], s);
+                y[r] = s;
+            }
+#pragma unroll
+            for (int q = 0; q < K; ++q) carry[(c * KC + q) * TL + l] = y[q];
+        }
+        __syncthreads();
+    }
+}
+
 // Steps 1-4 of a build: gather the right-hand side rows (spline_builder.hpp:952-1052), forward and
 // backward sweeps, border correction. On return (after a barrier) T[j*TL + l] holds solution
 // column j of line l, for j < n.
@@ -128,20 +167,23 @@ __device__ __forceinline__ void solve_tile(BuildArgs const& args, double* smem)
     int64_t const line = (int64_t)blockIdx.x * TL + l;
     bool const live = line < args.nlines;
 
-    // ---- 1. gather the right-hand side: values by async copies, Hermite rows scaled by dx^k ----
+    // ---- 1. gather the right-hand side: tile row r holds system row (r + lrot) mod n; values
+    //         arrive by async copies, Hermite rows are scaled by dx^k ----
     {
         int64_t const ov = live ? line_offset(args.lv, line) : 0;
         int const v0 = (args.raw || R.periodic) ? 0 : R.nbe_lo;
         int const v1 = (args.raw || R.periodic) ? n : R.nbe_lo + R.npoints;
         for (int r = c; r < n; r += nct) {
-            if (live && r >= v0 && r < v1) {
-                cp_async8(T + r * TL + l, args.vals + (int64_t)(r - v0) * args.lv.stride + ov);
+            int sr = r + R.lrot;
+            sr -= (sr >= n) ? n : 0;
+            if (live && sr >= v0 && sr < v1) {
+                cp_async8(T + r * TL + l, args.vals + (int64_t)(sr - v0) * args.lv.stride + ov);
             } else {
                 double v = 0.0;
-                if (live && r < R.nbe_lo) {
-                    if (r < R.nbv_lo) v = args.dlo[r * args.llo.stride + line_offset(args.llo, line)] * R.dxpow_lo[r];
-                } else if (live && r >= v1) {
-                    int const i = r - (n - R.nbe_hi);
+                if (live && sr < R.nbe_lo) {
+                    if (sr < R.nbv_lo) v = args.dlo[sr * args.llo.stride + line_offset(args.llo, line)] * R.dxpow_lo[sr];
+                } else if (live && sr >= v1) {
+                    int const i = sr - (n - R.nbe_hi);
                     if (i < R.nbv_hi) v = args.dhi[i * args.lhi.stride + line_offset(args.lhi, line)] * R.dxpow_hi[i];
                 }
                 T[r * TL + l] = v;
@@ -173,34 +215,12 @@ __device__ __forceinline__ void solve_tile(BuildArgs const& args, double* smem)
             }
         }
         __syncthreads();
-        if (c == 0) {
-            double cin[KL];
-#pragma unroll
-            for (int q = 0; q < KL; ++q) cin[q] = 0.0;
-            for (int cc = 0; cc < NC; ++cc) {
-                double hat[KL];
-#pragma unroll
-                for (int q = 0; q < KL; ++q) {
-                    hat[q] = carry[(cc * KC + q) * TL + l];
-                    carry[(cc * KC + q) * TL + l] = cin[q];
-                }
-                double const* P = t.PhiF + (size_t)cc * KL * KL;
-#pragma unroll
-                for (int r = 0; r < KL; ++r) {
-                    double s = hat[r];
-#pragma unroll
-                    for (int q = 0; q < KL; ++q) s = fma(__ldg(P + r * KL + q), cin[q], s);
-                    hat[r] = s;
-                }
-#pragma unroll
-                for (int q = 0; q < KL; ++q) cin[q] = hat[q];
-            }
-        }
-        __syncthreads();
+        carry_scan<KL, KC, TL, true>(t.PhiF, carry, t.nscan, NC, c, l);
         if (c < NC) {
             double w[KL + 1];
 #pragma unroll
-            for (int q = 0; q < KL; ++q) w[q] = (a + q < m) ? T[(a + q) * TL + l] + carry[(c * KC + q) * TL + l] : 0.0;
+            for (int q = 0; q < KL; ++q)
+                w[q] = (a + q < m) ? T[(a + q) * TL + l] + (c > 0 ? carry[((c - 1) * KC + q) * TL + l] : 0.0) : 0.0;
             if (t.pivot) fwd_sweep<KL, true>(t, T, TL, l, a, e, w, true, halo + (size_t)c * KL * TL + l, TL);
             else fwd_sweep<KL, false>(t, T, TL, l, a, e, w, true, halo + (size_t)c * KL * TL + l, TL);
         }
@@ -216,34 +236,11 @@ __device__ __forceinline__ void solve_tile(BuildArgs const& args, double* smem)
             for (int q = 0; q < KU; ++q) carry[(c * KC + q) * TL + l] = z[q];
         }
         __syncthreads();
-        if (c == 0) {
-            double cin[KU];
-#pragma unroll
-            for (int q = 0; q < KU; ++q) cin[q] = 0.0;
-            for (int cc = NC - 1; cc >= 0; --cc) {
-                double hat[KU];
-#pragma unroll
-                for (int q = 0; q < KU; ++q) {
-                    hat[q] = carry[(cc * KC + q) * TL + l];
-                    carry[(cc * KC + q) * TL + l] = cin[q];
-                }
-                double const* P = t.PhiB + (size_t)cc * KU * KU;
-#pragma unroll
-                for (int r = 0; r < KU; ++r) {
-                    double s = hat[r];
-#pragma unroll
-                    for (int q = 0; q < KU; ++q) s = fma(__ldg(P + r * KU + q), cin[q], s);
-                    hat[r] = s;
-                }
-#pragma unroll
-                for (int q = 0; q < KU; ++q) cin[q] = hat[q];
-            }
-        }
-        __syncthreads();
+        carry_scan<KU, KC, TL, false>(t.PhiB, carry, t.nscan, NC, c, l);
         if (c < NC) {
             double z[KU];
 #pragma unroll
-            for (int q = 0; q < KU; ++q) z[q] = carry[(c * KC + q) * TL + l];
+            for (int q = 0; q < KU; ++q) z[q] = (c + 1 < NC) ? carry[((c + 1) * KC + q) * TL + l] : 0.0;
             bwd_sweep<KU>(t, T, TL, l, a, e, z, true);
         }
         __syncthreads();
@@ -251,15 +248,18 @@ __device__ __forceinline__ void solve_tile(BuildArgs const& args, double* smem)
 
     // ---- 4. border: x2 = S^-1 (b2 - lambda x'), x1 = x' - (Q^-1 gamma) x2 ----
     if (k > 0) {
-        if (c == 0) {
-            for (int r = 0; r < k; ++r) btmp[r * TL + l] = T[(m + r) * TL + l];
-            for (int q = 0; q < t.lam_nnz; ++q)
-                btmp[__ldg(t.lam_row + q) * TL + l] -= __ldg(t.lam_val + q) * T[__ldg(t.lam_col + q) * TL + l];
-            for (int r = 0; r < k; ++r) {
-                double s = 0.0;
-                for (int q = 0; q < k; ++q) s = fma(__ldg(t.Sinv + r * k + q), btmp[q * TL + l], s);
-                T[(m + r) * TL + l] = s;
-            }
+        // border row r is handled by chunk thread r of the line
+        for (int r = c; r < k; r += nct) {
+            double s = T[(m + r) * TL + l];
+            int const q1 = __ldg(t.lam_row + r + 1);
+            for (int q = __ldg(t.lam_row + r); q < q1; ++q) s = fma(-__ldg(t.lam_val + q), T[__ldg(t.lam_col + q) * TL + l], s);
+            btmp[r * TL + l] = s;
+        }
+        __syncthreads();
+        for (int r = c; r < k; r += nct) {
+            double s = 0.0;
+            for (int q = 0; q < k; ++q) s = fma(__ldg(t.Sinv + r * k + q), btmp[q * TL + l], s);
+            T[(m + r) * TL + l] = s;
         }
         __syncthreads();
         int const nq = t.qg_lo + t.qg_hi;
@@ -273,14 +273,14 @@ __device__ __forceinline__ void solve_tile(BuildArgs const& args, double* smem)
     }
 }
 
-// Tile row holding the coefficient of B-spline b (spline_builder.hpp:1061-1100: the solution of
-// column j is the coefficient of B-spline j + offset, and the periodic rows n.. repeat rows 0..).
+// Tile row holding output row b: the solution of tile column j belongs to B-spline
+// (j + srot) mod n (srot combines the periodic offset of spline_builder.hpp:619-658 with the
+// rotation of the boundary blocks), and periodic rows n.. repeat rows 0.. (spline_builder.hpp:1073-1100).
 __device__ __forceinline__ int coef_row(RhsMap const& R, int n, int b)
 {
-    if (!R.periodic) return b;
-    int r = (b >= n ? b - n : b) - R.offset;
-    if (r < 0) r += n;
-    if (r >= n) r -= n;
+    int r = (b >= n ? b - n : b) - R.srot;
+    r += (r < 0) ? n : 0;
+    r -= (r >= n) ? n : 0;
     return r;
 }
 
@@ -296,10 +296,7 @@ __device__ __forceinline__ void store_tile(BuildArgs const& args, const double* 
     if (line >= args.nlines) return;
     int64_t const oo = line_offset(args.lo, line);
     int const rows = args.raw ? n : args.r.size;
-    for (int r = c; r < rows; r += args.nct) {
-        int const src = args.raw ? r : coef_row(args.r, n, r);
-        args.out[r * args.lo.stride + oo] = T[src * TL + l];
-    }
+    for (int r = c; r < rows; r += args.nct) args.out[r * args.lo.stride + oo] = T[coef_row(args.r, n, r) * TL + l];
 }
 
 } // namespace ddcb

@@ -51,15 +51,17 @@ void launch_k(BuildArgs const& args, int TL, cudaStream_t s)
 void dispatch(BuildArgs const& args, int TL, cudaStream_t s)
 {
     int const kl = args.t.kl, ku = args.t.ku;
-    // the plan pads kl to 1, 2 or 4 and ku to 1, 2, 4 or 8 with ku >= kl (plan.cpp, analyse)
+    // the plan pads (kl, ku) up to one of these shapes (plan.cpp, HostSolve::analyse)
     if (kl == 1 && ku == 1) launch_k<1, 1>(args, TL, s);
     else if (kl == 1 && ku == 2) launch_k<1, 2>(args, TL, s);
-    else if (kl == 1 && ku == 4) launch_k<1, 4>(args, TL, s);
-    else if (kl == 1 && ku == 8) launch_k<1, 8>(args, TL, s);
     else if (kl == 2 && ku == 2) launch_k<2, 2>(args, TL, s);
+    else if (kl == 3 && ku == 3) launch_k<3, 3>(args, TL, s);
+    else if (kl == 1 && ku == 4) launch_k<1, 4>(args, TL, s);
     else if (kl == 2 && ku == 4) launch_k<2, 4>(args, TL, s);
-    else if (kl == 2 && ku == 8) launch_k<2, 8>(args, TL, s);
     else if (kl == 4 && ku == 4) launch_k<4, 4>(args, TL, s);
+    else if (kl == 3 && ku == 6) launch_k<3, 6>(args, TL, s);
+    else if (kl == 1 && ku == 8) launch_k<1, 8>(args, TL, s);
+    else if (kl == 2 && ku == 8) launch_k<2, 8>(args, TL, s);
     else if (kl == 4 && ku == 8) launch_k<4, 8>(args, TL, s);
     else throw Error(DDCB_ERR_UNSUPPORTED, "band shape kl=" + std::to_string(kl) + " ku=" + std::to_string(ku) + " has no kernel");
 }
@@ -110,6 +112,8 @@ bool launch_build_eval(Builder const& b, Evaluator const& e, int order, double* 
     bool fused = false;
     if (b.tile_lines == 8 && b.precision == DDCB_FP64) {
         BuildArgs args = make_build_args(b, coefs, lc, vals, lv, dlo, llo, dhi, lhi);
+        // the evaluation part uses every thread: 64 point threads per line (512 per block)
+        args.nct = std::max(args.nct, 64);
         fused = launch_build_eval_fused(args, e, order, out, lo, coords, lx, s);
     }
     if (!fused) {
@@ -146,6 +150,10 @@ void launch_solve_multirhs(Builder const& b, double* rhs, long ld, long nrhs, bo
     args.t = transpose ? b.tables_t : b.tables;
     args.r = b.rhs;
     args.raw = 1;
+    // A x = b: rows enter rotated by rrot, the solution leaves rotated by crot; A^T swaps the two
+    args.r.lrot = transpose ? b.crot : b.rrot;
+    args.r.srot = transpose ? b.rrot : b.crot;
+    args.r.periodic = 0;
     args.nlines = nrhs;
     Lines L {b.n, ld, nrhs, 1, 0};
     args.vals = rhs;

@@ -50,14 +50,15 @@ struct SolveTables
     int pivot;       // 1 if any row interchange happened
     int nchunk;      // chunks per line used by the sweeps
     int chunk_len;   // every chunk but the last has this (odd) length; the last absorbs the rest
+    int nscan;       // steps of the log-depth carry scan: ceil(log2(nchunk))
     const double* Lf;    // m x kl: Lf[j*kl + t-1] = multiplier of row j+t at step j
     const int8_t* piv;   // m: pivot row offset at step j (ipiv[j] - j)
     const double* Uf;    // m x (ku+1): [1/U_jj, U_j,j+1 .. U_j,j+ku]
-    const double* PhiF;  // nchunk x kl x kl forward carry transfer
-    const double* PhiB;  // nchunk x ku x ku backward carry transfer
+    const double* PhiF;  // nscan x nchunk x kl x kl: transfer over chunks c-2^k+1..c (forward)
+    const double* PhiB;  // nscan x nchunk x ku x ku: transfer over chunks c..c+2^k-1 (backward)
     // border (k > 0)
     int lam_nnz;
-    const int* lam_row;
+    const int* lam_row;   // k+1 row pointers into lam_col / lam_val
     const int* lam_col;
     const double* lam_val;
     const double* Sinv;  // k x k inverse of the Schur complement S0 - l Q^-1 g
@@ -72,6 +73,8 @@ struct RhsMap
     int nbv_lo, nbv_hi;   // of which read from the derivative inputs (0 for homogeneous Hermite)
     int npoints;          // interpolation values
     int offset;           // periodic column rotation (spline_builder.hpp:619-658)
+    int lrot;             // tile row r holds right-hand side row (r + lrot) mod n
+    int srot;             // output row o (o < n) is tile row (o - srot) mod n; rows >= n repeat
     int size;             // coefficient rows (nbasis + degree)
     int periodic;
     double dxpow_lo[8];   // dx^(i+odd) for the Hermite rows
@@ -100,6 +103,7 @@ struct Builder
     int lo = 0, hi = 0;
     int nbe_lo = 0, nbe_hi = 0, nbv_lo = 0, nbv_hi = 0, odd = 0;
     int offset = 0;
+    int rrot = 0, crot = 0;  // rotation of rows / columns into the kernel's order (boundary blocks last)
     double dx = 0.0;
     long n = 0;             // nbasis
     std::vector<double> points;
@@ -145,6 +149,11 @@ void free_basis(Basis& b);
 std::vector<double> greville_points(Basis const& b, int lo, int hi);
 void basis_integrals(Basis const& b, double* out);
 Builder* create_builder(Basis const& basis, double const* pts, long npts, int lo, int hi, ddcb_builder_options const* opts);
+// host part of create_builder (no CUDA call) and the device upload it is followed by
+Builder* create_builder_host(Basis const& basis, double const* pts, long npts, int lo, int hi, ddcb_builder_options const* opts);
+void upload_builder(Builder* b);
+double emulate_device_solve(Builder const& b, double const* rhs, bool transpose);
+double emulate_build(Builder const& b, double const* vals, double const* dlo, double const* dhi);
 void destroy_builder(Builder* b);
 void builder_quadrature(Builder const& b, double* qlo, double* q, double* qhi);
 

@@ -18,26 +18,35 @@ struct EvalBasis
 
 #if defined(__CUDACC__)
 
-// Coefficient of B-spline b of one line: C[b*cs] (coefficients stored in basis order).
+// Coefficient access of one line. row0(jmin) gives the row of B-spline jmin; get(row0, i) the
+// coefficient of B-spline jmin + i.
+// CoefDirect: coefficients in basis order, row b at C[b*cs].
 struct CoefDirect
 {
     const double* C;
     int cs;
-    __device__ __forceinline__ double operator()(int b) const { return C[b * cs]; }
+    __device__ __forceinline__ int row0(int jmin) const { return jmin; }
+    __device__ __forceinline__ double get(int r0, int i) const { return C[(r0 + i) * cs]; }
 };
 
-// Coefficients still in the builder's column order inside its tile: B-spline b lives in column
-// (b mod n) - offset (mod n) (spline_builder.hpp:1061-1100).
+// CoefRotated: coefficients still in the builder's column order inside its tile: B-spline b lives
+// in column ((b mod n) - offset) mod n (spline_builder.hpp:1061-1100).
 struct CoefRotated
 {
     const double* C;
     int cs;
     int n;
     int offset;
-    __device__ __forceinline__ double operator()(int b) const
+    __device__ __forceinline__ int row0(int jmin) const
     {
-        int r = (b >= n ? b - n : b) - offset;
+        int r = jmin - offset;
         r += (r < 0) ? n : 0;
+        r -= (r >= n) ? n : 0;
+        return r;
+    }
+    __device__ __forceinline__ double get(int r0, int i) const
+    {
+        int r = r0 + i;
         r -= (r >= n) ? n : 0;
         return C[r * cs];
     }
@@ -77,9 +86,10 @@ __device__ __forceinline__ double eval_value_no_bc(EvalBasis const& eb, double x
         nonuniform_values_t<D>(eb.b.knots, eb.inv_span, eb.nk, ck, x, v);
         jmin = ck - D;
     }
+    int const r0 = C.row0(jmin);
     double y = 0.0;
 #pragma unroll
-    for (int i = 0; i < D + 1; ++i) y = fma(C(jmin + i), v[i], y);
+    for (int i = 0; i < D + 1; ++i) y = fma(C.get(r0, i), v[i], y);
     return y;
 }
 
@@ -121,8 +131,10 @@ __device__ __forceinline__ double eval_deriv_no_bc(EvalBasis const& eb, double x
         nonuniform_values_t<P>(eb.b.knots, eb.inv_span, eb.nk, ck, x, v);
         jmin = ck - D;
     }
+    const double* ispan = eb.inv_span + jmin; // knot-span inverses starting at knot jmin
+    int const r0 = C.row0(jmin);
 #pragma unroll
-    for (int i = 0; i < D + 1; ++i) cc[i] = C(jmin + i);
+    for (int i = 0; i < D + 1; ++i) cc[i] = C.get(r0, i);
 #pragma unroll
     for (int k = 1; k <= ORDER; ++k) {
 #pragma unroll
@@ -131,7 +143,7 @@ __device__ __forceinline__ double eval_deriv_no_bc(EvalBasis const& eb, double x
                 cc[i] = (cc[i] - cc[i - 1]) * eb.b.inv_step;
             } else {
                 // c^(k)_j = (D-k+1) (c_j - c_{j-1}) / (t_{j+D-k+1} - t_j), j = jmin + i
-                cc[i] = double(D - k + 1) * (cc[i] - cc[i - 1]) * __ldg(eb.inv_span + (D - k) * eb.nk + jmin + i);
+                cc[i] = double(D - k + 1) * (cc[i] - cc[i - 1]) * __ldg(ispan + (D - k) * eb.nk + i);
             }
         }
     }

@@ -42,8 +42,10 @@ __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src)
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
 }
 
+constexpr int kEvalThreads = 512;
+
 template <int D, int TLE, int ORDER, bool UNI>
-__global__ void __launch_bounds__(256) eval_kernel(const __grid_constant__ EvalArgs a)
+__global__ void __launch_bounds__(kEvalThreads) eval_kernel(const __grid_constant__ EvalArgs a)
 {
     extern __shared__ double smem[];
     double* C = smem;                                  // size x TLE coefficient tile
@@ -69,28 +71,25 @@ __global__ void __launch_bounds__(256) eval_kernel(const __grid_constant__ EvalA
     int64_t const oo = line_offset(a.lo, line);
     int64_t const m = a.lx.n;
     CoefDirect const acc {C + l, TLE};
-    const double* __restrict__ coords = a.coords;
-    double* __restrict__ out = a.out;
-    constexpr int U = 4; // points in flight per thread
-    for (int64_t p0 = c; p0 < m; p0 += (int64_t)U * nct) {
+    constexpr int U = 8; // points in flight per thread
+    int64_t const sx = a.lx.stride * nct, so = a.lo.stride * nct;
+    const double* __restrict__ xp = a.coords + ox + c * a.lx.stride;
+    double* __restrict__ op = a.out + oo + c * a.lo.stride;
+    int const npt = m > c ? int((m - c + nct - 1) / nct) : 0; // points of this thread
+    for (int q0 = 0; q0 < npt; q0 += U) {
         double xs[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            int64_t const p = p0 + (int64_t)u * nct;
-            xs[u] = p < m ? coords[p * a.lx.stride + ox] : 0.0;
-        }
+        for (int u = 0; u < U; ++u) xs[u] = (q0 + u < npt) ? xp[(q0 + u) * sx] : 0.0;
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            int64_t const p = p0 + (int64_t)u * nct;
-            if (p < m) out[p * a.lo.stride + oo] = eval_point<D, ORDER, UNI>(eb, a.ex_lo, a.ex_hi, xs[u], acc);
-        }
+        for (int u = 0; u < U; ++u)
+            if (q0 + u < npt) op[(q0 + u) * so] = eval_point<D, ORDER, UNI>(eb, a.ex_lo, a.ex_hi, xs[u], acc);
     }
 }
 
 template <int D, int TLE, bool UNI>
 void launch_order(EvalArgs const& a, int order, size_t sm, cudaStream_t s)
 {
-    dim3 grid((unsigned)((a.nlines + TLE - 1) / TLE)), block(256);
+    dim3 grid((unsigned)((a.nlines + TLE - 1) / TLE)), block(kEvalThreads);
 #define DDCB_EVAL_CASE(O)                                                                                  \
     case O:                                                                                                \
         if constexpr (O <= D) {                                                                            \

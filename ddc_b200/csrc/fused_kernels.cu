@@ -44,22 +44,19 @@ __global__ void __launch_bounds__(1024) build_eval_kernel(const __grid_constant_
     int64_t const ox = line_offset(fe.lx, line);
     int64_t const oo = line_offset(fe.lo, line);
     int64_t const m = fe.lx.n;
-    CoefRotated const acc {smem + l, TL, args.t.n, args.r.periodic ? args.r.offset : 0};
-    const double* __restrict__ coords = fe.coords;
-    double* __restrict__ out = fe.out;
-    constexpr int U = 4;
-    for (int64_t p0 = c; p0 < m; p0 += (int64_t)U * nct) {
+    CoefRotated const acc {smem + l, TL, args.t.n, args.r.srot};
+    constexpr int U = 8; // points in flight per thread
+    int64_t const sx = fe.lx.stride * nct, so = fe.lo.stride * nct;
+    const double* __restrict__ xp = fe.coords + ox + c * fe.lx.stride;
+    double* __restrict__ op = fe.out + oo + c * fe.lo.stride;
+    int const npt = m > c ? int((m - c + nct - 1) / nct) : 0; // points of this thread
+    for (int q0 = 0; q0 < npt; q0 += U) {
         double xs[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            int64_t const p = p0 + (int64_t)u * nct;
-            xs[u] = p < m ? coords[p * fe.lx.stride + ox] : 0.0;
-        }
+        for (int u = 0; u < U; ++u) xs[u] = (q0 + u < npt) ? xp[(q0 + u) * sx] : 0.0;
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            int64_t const p = p0 + (int64_t)u * nct;
-            if (p < m) out[p * fe.lo.stride + oo] = eval_point<D, ORDER, UNI>(eb, fe.ex_lo, fe.ex_hi, xs[u], acc);
-        }
+        for (int u = 0; u < U; ++u)
+            if (q0 + u < npt) op[(q0 + u) * so] = eval_point<D, ORDER, UNI>(eb, fe.ex_lo, fe.ex_hi, xs[u], acc);
     }
 }
 
@@ -120,6 +117,7 @@ bool launch_build_eval_fused(BuildArgs const& args, Evaluator const& e, int orde
     int const kl = args.t.kl, ku = args.t.ku;
     if (kl == 1 && ku == 1) return launch_deg<1, 1>(args, fe, order, s);
     if (kl == 2 && ku == 2) return launch_deg<2, 2>(args, fe, order, s);
+    if (kl == 3 && ku == 3) return launch_deg<3, 3>(args, fe, order, s);
     if (kl == 4 && ku == 4) return launch_deg<4, 4>(args, fe, order, s);
     return false;
 }

@@ -228,7 +228,7 @@ struct BandLU
     double& at(long i, long j) { return w[(kl + ku + i - j) * m + j]; }
     double at(long i, long j) const { return w[(kl + ku + i - j) * m + j]; }
 
-    void factor()
+    void factor(bool pivoting = true)
     {
         ipiv.assign(m, 0);
         long ju = 0;
@@ -236,7 +236,7 @@ struct BandLU
             long const km = std::min(kl, m - 1 - j);
             long jp = 0;
             double amax = std::fabs(at(j, j));
-            for (long t = 1; t <= km; ++t)
+            for (long t = 1; t <= km && pivoting; ++t)
                 if (std::fabs(at(j + t, j)) > amax) {
                     amax = std::fabs(at(j + t, j));
                     jp = t;
@@ -337,7 +337,7 @@ struct HostSolve
     long kl = 0, ku = 0;       // effective L / U bandwidths
     bool pivot = false;
     // chunking
-    long nchunk = 1, chunk_len = 0;
+    long nchunk = 1, chunk_len = 0, nscan = 0;
     std::vector<double> Lf, Uf, PhiF, PhiB;
     std::vector<int8_t> piv;
     long qg_lo = 0, qg_hi = 0;
@@ -348,11 +348,13 @@ struct HostSolve
     long chunk_begin(long c) const { return c * chunk_len; }
     long chunk_end(long c) const { return (c == nchunk - 1) ? m : (c + 1) * chunk_len; }
 
-    void analyse(SparseRows const& rows, bool periodic)
+    // rows: the system in kernel order (the builder rotates the reference's boundary rows and
+    // columns to the end); border: the number of trailing rows/cols solved through the Schur
+    // complement (periodic systems: derived from the circular bandwidth instead).
+    void analyse(SparseRows const& rows, bool periodic, long border)
     {
         n = long(rows.size());
-        // Border: periodic systems couple the ends; the circular bandwidth sets the border size.
-        k = 0;
+        k = border;
         if (periodic) {
             long bl = 0, bu = 0;
             for (long i = 0; i < n; ++i)
@@ -389,7 +391,38 @@ struct HostSolve
                 else if (j < m) lam[(i - m) * m + j] = v;
                 else delta[(i - m) * k + (j - m)] = v;
             }
-        if (m > 0) lu.factor();
+        // Factorise without interchanges when that is as accurate as partial pivoting (the
+        // interpolation block of B-spline collocation matrices is totally positive, for which
+        // elimination without pivoting is stable: de Boor & Pinkus 1977); else pivot.
+        if (m > 0) {
+            BandLU piv_lu = lu;
+            piv_lu.factor(true);
+            bool use_nopiv = true;
+            try {
+                lu.factor(false);
+            } catch (Error const&) {
+                use_nopiv = false;
+            }
+            if (use_nopiv) {
+                std::vector<double> x1(m), x2(m);
+                unsigned long long st = 0x9E3779B97F4A7C15ULL;
+                for (int trial = 0; trial < 3 && use_nopiv; ++trial) {
+                    for (long i = 0; i < m; ++i) {
+                        st = st * 6364136223846793005ULL + 1442695040888963407ULL;
+                        x1[i] = x2[i] = double(st >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+                    }
+                    lu.solve(x1.data(), false);
+                    piv_lu.solve(x2.data(), false);
+                    double num = 0.0, den = 0.0;
+                    for (long i = 0; i < m; ++i) {
+                        num = std::max(num, std::fabs(x1[i] - x2[i]));
+                        den = std::max(den, std::fabs(x2[i]));
+                    }
+                    if (!(num <= 1e-14 * den)) use_nopiv = false;
+                }
+            }
+            if (!use_nopiv) lu = piv_lu;
+        }
         // Q^-1 gamma
         std::vector<double> col(m);
         for (long r = 0; r < k; ++r) {
@@ -415,26 +448,29 @@ struct HostSolve
             for (long t = 1; t <= lu.kl + lu.ku && j + t < m; ++t)
                 if (lu.at(j, j + t) != 0.0) ku = std::max(ku, t);
         }
-        // pad the bandwidths up to the shapes the kernels are compiled for (build_kernels.cu)
-        auto up = [](long v, std::initializer_list<long> menu) {
-            for (long x : menu)
-                if (v <= x) return x;
-            return -1L;
-        };
-        long const klp = up(std::max(kl, 1L), {1, 2, 4});
-        long kup = up(std::max(ku, 1L), {1, 2, 4, 8});
-        if (klp < 0 || kup < 0)
+        // pad the bandwidths up to the cheapest band shape the kernels are compiled for
+        // (build_kernels.cu dispatch)
+        static long const shapes[][2] = {{1, 1}, {1, 2}, {2, 2}, {3, 3}, {1, 4}, {2, 4}, {4, 4}, {3, 6}, {1, 8}, {2, 8}, {4, 8}};
+        long best = -1;
+        for (long i = 0; i < long(sizeof(shapes) / sizeof(shapes[0])); ++i)
+            if (shapes[i][0] >= std::max(kl, 1L) && shapes[i][1] >= std::max(ku, 1L)) {
+                best = i;
+                break;
+            }
+        if (best < 0)
             throw Error(DDCB_ERR_UNSUPPORTED, "band too wide for the device solver (kl=" + std::to_string(kl) + ", ku=" + std::to_string(ku) + ")");
-        kl = klp;
-        ku = std::max(kup, klp);
-        // lambda in COO form
-        for (long i = 0; i < k; ++i)
+        kl = shapes[best][0];
+        ku = shapes[best][1];
+        // lambda in compressed-row form (row i of the border: entries lam_ptr[i]..lam_ptr[i+1])
+        lam_row.assign(1, 0);
+        for (long i = 0; i < k; ++i) {
             for (long j = 0; j < m; ++j)
                 if (lam[i * m + j] != 0.0) {
-                    lam_row.push_back(int(i));
                     lam_col.push_back(int(j));
                     lam_val.push_back(lam[i * m + j]);
                 }
+            lam_row.push_back(int(lam_val.size()));
+        }
         // rows of Q^-1 gamma that matter (the correction decays away from the ends)
         double gmax = 0.0;
         for (double v : gam) gmax = std::max(gmax, std::fabs(v));
@@ -519,8 +555,8 @@ struct HostSolve
             if (nchunk == 1) L = m;
             chunk_len = L;
         }
-        PhiF.assign(std::max<long>(nchunk * kl * kl, 1), 0.0);
-        PhiB.assign(std::max<long>(nchunk * ku * ku, 1), 0.0);
+        // transfer matrices of one chunk: Phi_c (forward, kl x kl), Psi_c (backward, ku x ku)
+        std::vector<double> F(std::max<long>(nchunk * kl * kl, 1), 0.0), G(std::max<long>(nchunk * ku * ku, 1), 0.0);
         std::vector<double> w(std::max<long>(kl, 1)), z(std::max<long>(ku, 1));
         for (long c = 0; c < nchunk && m > 0; ++c) {
             long const a = chunk_begin(c), e = chunk_end(c);
@@ -528,13 +564,44 @@ struct HostSolve
                 std::fill(w.begin(), w.end(), 0.0);
                 w[s] = 1.0;
                 fwd_steps(a, e, w.data());
-                for (long r = 0; r < kl; ++r) PhiF[(c * kl + r) * kl + s] = w[r];
+                for (long r = 0; r < kl; ++r) F[(c * kl + r) * kl + s] = w[r];
             }
             for (long s = 0; s < ku; ++s) {
                 std::fill(z.begin(), z.end(), 0.0);
                 z[s] = 1.0;
                 bwd_steps(a, e, z.data());
-                for (long r = 0; r < ku; ++r) PhiB[(c * ku + r) * ku + s] = z[r];
+                for (long r = 0; r < ku; ++r) G[(c * ku + r) * ku + s] = z[r];
+            }
+        }
+        // Products over runs of 2^k chunks for the log-depth carry scan (build_device.cuh):
+        //   forward  P(k, c) = Phi_c Phi_{c-1} ... Phi_{c-2^k+1}
+        //   backward Q(k, c) = Psi_c Psi_{c+1} ... Psi_{c+2^k-1}
+        nscan = 0;
+        while ((1L << nscan) < nchunk) ++nscan;
+        PhiF.assign(std::max<long>(nscan * nchunk * kl * kl, 1), 0.0);
+        PhiB.assign(std::max<long>(nscan * nchunk * ku * ku, 1), 0.0);
+        auto matmul = [](double const* A, double const* B, double* C, long n) {
+            for (long i = 0; i < n; ++i)
+                for (long j = 0; j < n; ++j) {
+                    double acc = 0.0;
+                    for (long q = 0; q < n; ++q) acc += A[i * n + q] * B[q * n + j];
+                    C[i * n + j] = acc;
+                }
+        };
+        for (long k = 0; k < nscan; ++k) {
+            long const half = (1L << k) / 2;
+            for (long c = 0; c < nchunk; ++c) {
+                double* Pf = &PhiF[(k * nchunk + c) * kl * kl];
+                double* Pb = &PhiB[(k * nchunk + c) * ku * ku];
+                if (k == 0) {
+                    std::copy(&F[c * kl * kl], &F[(c + 1) * kl * kl], Pf);
+                    std::copy(&G[c * ku * ku], &G[(c + 1) * ku * ku], Pb);
+                    continue;
+                }
+                if (c - (1L << k) + 1 >= 0)
+                    matmul(&PhiF[((k - 1) * nchunk + c) * kl * kl], &PhiF[((k - 1) * nchunk + c - half) * kl * kl], Pf, kl);
+                if (c + (1L << k) - 1 <= nchunk - 1)
+                    matmul(&PhiB[((k - 1) * nchunk + c) * ku * ku], &PhiB[((k - 1) * nchunk + c + half) * ku * ku], Pb, ku);
             }
         }
     }
@@ -641,6 +708,7 @@ SolveTables upload_tables(HostSolve const& h, std::vector<char>& blob, std::vect
     t.pivot = h.pivot ? 1 : 0;
     t.nchunk = int(h.nchunk);
     t.chunk_len = int(h.chunk_len);
+    t.nscan = int(h.nscan);
     t.lam_nnz = int(h.lam_val.size());
     t.qg_lo = int(h.qg_lo);
     t.qg_hi = int(h.qg_hi);
@@ -722,9 +790,10 @@ static void check_valid_grid(Builder const& b)
 struct BuilderPrivate
 {
     HostSolve fwd, adj;
+    SparseRows ref_rows; // the assembled system in the reference's row / column order
 };
 
-Builder* create_builder(Basis const& basis, double const* pts, long npts, int lo, int hi, ddcb_builder_options const* opts)
+Builder* create_builder_host(Basis const& basis, double const* pts, long npts, int lo, int hi, ddcb_builder_options const* opts)
 {
     if (pts == nullptr && npts > 0) throw Error(DDCB_ERR_INVALID_ARGUMENT, "interpolation points pointer is NULL");
     if (lo < 0 || lo > 3 || hi < 0 || hi > 3) throw Error(DDCB_ERR_INVALID_ARGUMENT, "unknown closure");
@@ -772,11 +841,35 @@ Builder* create_builder(Basis const& basis, double const* pts, long npts, int lo
             }
         }
         SparseRows rows = assemble(*b);
+        // Non-periodic systems: the reference's 3x3 block layout (splines_linear_problem_3x3_blocks.cpp,
+        // block sizes of spline_builder.hpp:668-709) -- the first `top` rows/cols (Hermite rows,
+        // Greville edge points) are rotated behind the band and, with the last `bottom`, form the
+        // border; the band in between is the interpolation block.
+        long top = 0, bottom = 0;
+        if (!D.periodic) {
+            auto block = [&](int bc, int nbc) -> long {
+                if (D.uniform) return (bc == DDCB_GREVILLE) ? d - 1 : nbc;
+                return (bc == DDCB_GREVILLE) ? d - 1 : nbc + 1;
+            };
+            top = block(lo, b->nbe_lo);
+            bottom = block(hi, b->nbe_hi);
+            if (top + bottom >= b->n) top = bottom = 0;
+        }
+        b->rrot = int(top);
+        b->crot = int(top);
+        if (top) {
+            long const nn = b->n;
+            SparseRows rot(nn);
+            for (long i = 0; i < nn; ++i)
+                for (auto const& [j, v] : rows[(i + top) % nn]) rot[i][modulo(j - top, nn)] = v;
+            rows.swap(rot);
+        }
         auto* priv = new BuilderPrivate();
         b->host_private = priv;
-        priv->fwd.analyse(rows, D.periodic != 0);
+        priv->ref_rows = assemble(*b);
+        priv->fwd.analyse(rows, D.periodic != 0, top + bottom);
         priv->fwd.make_tables(b->nchunk_req);
-        priv->adj.analyse(transpose_rows(rows), D.periodic != 0);
+        priv->adj.analyse(transpose_rows(rows), D.periodic != 0, top + bottom);
         priv->adj.make_tables(b->nchunk_req);
         b->k = int(priv->fwd.k);
         b->m = int(priv->fwd.m);
@@ -784,7 +877,13 @@ Builder* create_builder(Basis const& basis, double const* pts, long npts, int lo
         b->ku = int(priv->fwd.ku);
         b->pivot = priv->fwd.pivot ? 1 : 0;
         b->structure = describe(priv->fwd);
-        if (std::getenv("DDCB_DEBUG_PLAN")) std::fprintf(stderr, "ddcb plan: %s | adjoint %s\n", b->structure.c_str(), describe(priv->adj).c_str());
+        if (std::getenv("DDCB_DEBUG_PLAN")) {
+            std::fprintf(stderr, "ddcb plan: %s | adjoint %s\n", b->structure.c_str(), describe(priv->adj).c_str());
+            std::fprintf(stderr, "  swaps at:");
+            for (long j = 0; j < priv->fwd.m; ++j)
+                if (priv->fwd.lu.ipiv[j] != j) std::fprintf(stderr, " %ld->%d", j, priv->fwd.lu.ipiv[j]);
+            std::fprintf(stderr, "\n  lu.kl=%ld lu.ku=%ld\n", priv->fwd.lu.kl, priv->fwd.lu.ku);
+        }
         // right-hand side map
         RhsMap& r = b->rhs;
         r.nbe_lo = b->nbe_lo;
@@ -793,30 +892,253 @@ Builder* create_builder(Basis const& basis, double const* pts, long npts, int lo
         r.nbv_hi = b->nbv_hi;
         r.npoints = int(npts);
         r.offset = b->offset;
+        r.lrot = b->rrot;
+        r.srot = (b->offset + b->crot) % int(b->n);
         r.size = int(b->basis.size());
         r.periodic = D.periodic;
         for (int i = 0; i < 8; ++i) {
             r.dxpow_lo[i] = ipow(b->dx, i + b->odd);
             r.dxpow_hi[i] = ipow(b->dx, i + b->odd);
         }
-        // device tables (current device)
-        int dev = 0;
-        DDCB_CUDA_CHECK(cudaGetDevice(&dev));
-        b->device = dev;
-        upload_basis(b->basis, dev);
-        std::vector<char> blob;
-        std::vector<size_t> offs_f, offs_a;
-        b->tables = upload_tables(priv->fwd, blob, offs_f);
-        b->tables_t = upload_tables(priv->adj, blob, offs_a);
-        DDCB_CUDA_CHECK(cudaMalloc(&b->d_block, blob.size()));
-        DDCB_CUDA_CHECK(cudaMemcpy(b->d_block, blob.data(), blob.size(), cudaMemcpyHostToDevice));
-        b->d_block_bytes = blob.size();
-        bind_tables(b->tables, static_cast<char*>(b->d_block), offs_f.data());
-        bind_tables(b->tables_t, static_cast<char*>(b->d_block), offs_a.data());
         return b;
     } catch (...) {
         destroy_builder(b);
         throw;
+    }
+}
+
+void upload_builder(Builder* b)
+{
+    auto* priv = static_cast<BuilderPrivate*>(b->host_private);
+    int dev = 0;
+    DDCB_CUDA_CHECK(cudaGetDevice(&dev));
+    b->device = dev;
+    upload_basis(b->basis, dev);
+    std::vector<char> blob;
+    std::vector<size_t> offs_f, offs_a;
+    b->tables = upload_tables(priv->fwd, blob, offs_f);
+    b->tables_t = upload_tables(priv->adj, blob, offs_a);
+    DDCB_CUDA_CHECK(cudaMalloc(&b->d_block, blob.size()));
+    DDCB_CUDA_CHECK(cudaMemcpy(b->d_block, blob.data(), blob.size(), cudaMemcpyHostToDevice));
+    b->d_block_bytes = blob.size();
+    bind_tables(b->tables, static_cast<char*>(b->d_block), offs_f.data());
+    bind_tables(b->tables_t, static_cast<char*>(b->d_block), offs_a.data());
+}
+
+Builder* create_builder(Basis const& basis, double const* pts, long npts, int lo, int hi, ddcb_builder_options const* opts)
+{
+    Builder* b = create_builder_host(basis, pts, npts, lo, hi, opts);
+    try {
+        upload_builder(b);
+    } catch (...) {
+        destroy_builder(b);
+        throw;
+    }
+    return b;
+}
+
+// Runs, on the host, exactly the steps the device solve performs (chunked sweeps with the carry
+// scan, border correction) on one right-hand side and returns its max-norm distance to the direct
+// host solve, relative to the solution's max norm. Used by the host-side tests of the plan.
+static void emulate_tile_solve(HostSolve const& h, std::vector<double>& T);
+
+double emulate_device_solve(Builder const& b, double const* rhs, bool transpose)
+{
+    HostSolve const& h = transpose ? static_cast<BuilderPrivate const*>(b.host_private)->adj
+                                   : static_cast<BuilderPrivate const*>(b.host_private)->fwd;
+    long const n = h.n;
+    std::vector<double> T(rhs, rhs + n), ref(rhs, rhs + n);
+    h.solve_host(ref.data(), false); // h is already the transposed system when transpose is set
+    emulate_tile_solve(h, T);
+    double num = 0.0, den = 0.0;
+    for (long i = 0; i < n; ++i) {
+        num = std::max(num, std::fabs(T[i] - ref[i]));
+        den = std::max(den, std::fabs(ref[i]));
+    }
+    return num / std::max(den, 1e-300);
+}
+
+// Host replay of one device build of a single line: right-hand side gather with the row
+// rotation and Hermite scaling, tile solve, store with the column rotation and periodic copies.
+// Returns the max-norm distance (relative) to a dense Gaussian elimination of the system in the
+// reference's order followed by the reference's placement of the solution
+// (spline_builder.hpp:981-1100).
+double emulate_build(Builder const& b, double const* vals, double const* dlo, double const* dhi)
+{
+    auto const* priv = static_cast<BuilderPrivate const*>(b.host_private);
+    HostSolve const& h = priv->fwd;
+    RhsMap const& R = b.rhs;
+    long const n = b.n;
+    std::vector<double> T(n, 0.0);
+    bool const all_vals = R.periodic != 0;
+    long const v0 = all_vals ? 0 : R.nbe_lo, v1 = all_vals ? n : R.nbe_lo + R.npoints;
+    for (long r = 0; r < n; ++r) {
+        long const sr = (r + R.lrot) % n;
+        if (sr >= v0 && sr < v1) T[r] = vals[sr - v0];
+        else if (sr < R.nbe_lo) T[r] = sr < R.nbv_lo ? dlo[sr] * R.dxpow_lo[sr] : 0.0;
+        else {
+            long const i = sr - (n - R.nbe_hi);
+            T[r] = i < R.nbv_hi ? dhi[i] * R.dxpow_hi[i] : 0.0;
+        }
+    }
+    emulate_tile_solve(h, T);
+    std::vector<double> out(R.size);
+    for (long o = 0; o < R.size; ++o) {
+        long src = (o % n) - R.srot;
+        src = ((src % n) + n) % n;
+        out[o] = T[src];
+    }
+    // reference: dense system in reference order, rhs = [dlo*dx^k | vals | dhi*dx^k]
+    std::vector<double> A(n * n, 0.0), x(n, 0.0);
+    for (long i = 0; i < n; ++i)
+        for (auto const& [j, v] : priv->ref_rows[i]) A[i * n + j] = v;
+    for (long i = 0; i < n; ++i) {
+        if (all_vals) x[i] = vals[i];
+        else if (i < R.nbe_lo) x[i] = i < R.nbv_lo ? dlo[i] * R.dxpow_lo[i] : 0.0;
+        else if (i < R.nbe_lo + R.npoints) x[i] = vals[i - R.nbe_lo];
+        else {
+            long const q = i - (n - R.nbe_hi);
+            x[i] = q < R.nbv_hi ? dhi[q] * R.dxpow_hi[q] : 0.0;
+        }
+    }
+    for (long c = 0; c < n; ++c) { // Gaussian elimination with partial pivoting
+        long p = c;
+        for (long i = c + 1; i < n; ++i)
+            if (std::fabs(A[i * n + c]) > std::fabs(A[p * n + c])) p = i;
+        if (p != c) {
+            for (long j = 0; j < n; ++j) std::swap(A[c * n + j], A[p * n + j]);
+            std::swap(x[c], x[p]);
+        }
+        for (long i = c + 1; i < n; ++i) {
+            double const f = A[i * n + c] / A[c * n + c];
+            if (f == 0.0) continue;
+            for (long j = c; j < n; ++j) A[i * n + j] -= f * A[c * n + j];
+            x[i] -= f * x[c];
+        }
+    }
+    for (long c = n - 1; c >= 0; --c) {
+        double s = x[c];
+        for (long j = c + 1; j < n; ++j) s -= A[c * n + j] * x[j];
+        x[c] = s / A[c * n + c];
+    }
+    // column j of the reference system is B-spline (j + offset) mod n; rows n.. repeat rows 0..
+    std::vector<double> ref(R.size);
+    for (long j = 0; j < n; ++j) ref[(j + R.offset) % n] = x[j];
+    for (long o = n; o < R.size; ++o) ref[o] = ref[o - n];
+    double num = 0.0, den = 0.0;
+    for (long o = 0; o < R.size; ++o) {
+        num = std::max(num, std::fabs(out[o] - ref[o]));
+        den = std::max(den, std::fabs(ref[o]));
+    }
+    return num / std::max(den, 1e-300);
+}
+
+static void emulate_tile_solve(HostSolve const& h, std::vector<double>& T)
+{
+    long const m = h.m, k = h.k, KL = h.kl, KU = h.ku, NC = h.nchunk;
+    std::vector<double> carry(NC * std::max(KL, KU), 0.0), halo(NC * KL, 0.0);
+    auto scan = [&](std::vector<double> const& P, long K, bool fwd) {
+        std::vector<double> y(carry);
+        for (long s = 0; s < h.nscan; ++s) {
+            std::vector<double> next(y);
+            for (long c = 0; c < NC; ++c) {
+                long const nb = fwd ? c - (1L << s) : c + (1L << s);
+                if (nb < 0 || nb >= NC) continue;
+                double const* M = &P[(s * NC + c) * K * K];
+                for (long r = 0; r < K; ++r) {
+                    double acc = y[c * K + r];
+                    for (long q = 0; q < K; ++q) acc += M[r * K + q] * y[nb * K + q];
+                    next[c * K + r] = acc;
+                }
+            }
+            y = next;
+        }
+        carry = y;
+    };
+    if (m > 0) {
+        // forward, phase A
+        carry.assign(NC * KL, 0.0);
+        for (long c = 0; c < NC; ++c) {
+            long const a = h.chunk_begin(c), e = h.chunk_end(c);
+            std::vector<double> w(KL + 1, 0.0);
+            for (long q = 0; q < KL; ++q) w[q] = (a + q < m) ? T[a + q] : 0.0;
+            for (long j = a; j < e; ++j) {
+                w[KL] = (j + KL < m) ? T[j + KL] : 0.0;
+                long const p = h.piv[j];
+                if (p) std::swap(w[0], w[p]);
+                double const y = w[0];
+                for (long q = 1; q <= KL; ++q) w[q] -= h.Lf[j * KL + q - 1] * y;
+                for (long q = 0; q < KL; ++q) w[q] = w[q + 1];
+            }
+            for (long q = 0; q < KL; ++q) {
+                double const orig = (e + q < m) ? T[e + q] : 0.0;
+                carry[c * KL + q] = w[q] - orig;
+                halo[c * KL + q] = orig;
+            }
+        }
+        scan(h.PhiF, KL, true);
+        std::vector<double> Tn(T);
+        for (long c = 0; c < NC; ++c) {
+            long const a = h.chunk_begin(c), e = h.chunk_end(c);
+            std::vector<double> w(KL + 1, 0.0);
+            for (long q = 0; q < KL; ++q) w[q] = (a + q < m) ? T[a + q] + (c > 0 ? carry[(c - 1) * KL + q] : 0.0) : 0.0;
+            for (long j = a; j < e; ++j) {
+                long const rr = j + KL;
+                w[KL] = rr < e ? T[rr] : (rr < m ? halo[c * KL + rr - e] : 0.0);
+                long const p = h.piv[j];
+                if (p) std::swap(w[0], w[p]);
+                double const y = w[0];
+                Tn[j] = y;
+                for (long q = 1; q <= KL; ++q) w[q] -= h.Lf[j * KL + q - 1] * y;
+                for (long q = 0; q < KL; ++q) w[q] = w[q + 1];
+            }
+        }
+        T = Tn;
+        // backward
+        carry.assign(NC * KU, 0.0);
+        for (long c = 0; c < NC; ++c) {
+            long const a = h.chunk_begin(c), e = h.chunk_end(c);
+            std::vector<double> z(KU, 0.0);
+            for (long j = e - 1; j >= a; --j) {
+                double s = T[j];
+                for (long q = 1; q <= KU; ++q) s -= h.Uf[j * (KU + 1) + q] * z[q - 1];
+                double const x = s * h.Uf[j * (KU + 1)];
+                for (long q = KU - 1; q >= 1; --q) z[q] = z[q - 1];
+                z[0] = x;
+            }
+            for (long q = 0; q < KU; ++q) carry[c * KU + q] = z[q];
+        }
+        scan(h.PhiB, KU, false);
+        for (long c = 0; c < NC; ++c) {
+            long const a = h.chunk_begin(c), e = h.chunk_end(c);
+            std::vector<double> z(KU, 0.0);
+            for (long q = 0; q < KU; ++q) z[q] = (c + 1 < NC) ? carry[(c + 1) * KU + q] : 0.0;
+            for (long j = e - 1; j >= a; --j) {
+                double s = T[j];
+                for (long q = 1; q <= KU; ++q) s -= h.Uf[j * (KU + 1) + q] * z[q - 1];
+                double const x = s * h.Uf[j * (KU + 1)];
+                Tn[j] = x;
+                for (long q = KU - 1; q >= 1; --q) z[q] = z[q - 1];
+                z[0] = x;
+            }
+        }
+        T = Tn;
+    }
+    if (k > 0) {
+        std::vector<double> bt(k);
+        for (long r = 0; r < k; ++r) bt[r] = T[m + r];
+        for (long r = 0; r < k; ++r)
+            for (int q = h.lam_row[r]; q < h.lam_row[r + 1]; ++q) bt[r] -= h.lam_val[q] * T[h.lam_col[q]];
+        for (long r = 0; r < k; ++r) {
+            double s = 0.0;
+            for (long q = 0; q < k; ++q) s += h.Sinv[r * k + q] * bt[q];
+            T[m + r] = s;
+        }
+        long const nq = h.qg_lo + h.qg_hi;
+        for (long q = 0; q < nq; ++q) {
+            long const i = q < h.qg_lo ? q : m - h.qg_hi + (q - h.qg_lo);
+            for (long r = 0; r < k; ++r) T[i] -= h.qg_rows[q * k + r] * T[m + r];
+        }
     }
 }
 
@@ -838,9 +1160,13 @@ void builder_quadrature(Builder const& b, double* qlo, double* q, double* qhi)
     basis_integrals(b.basis, ints.data());
     // As the reference does, the right-hand side is integral_bsplines in basis order (entry j is
     // the integral of B-spline j), without the periodic column rotation.
-    std::vector<double> rhs(b.n);
-    for (long j = 0; j < b.n; ++j) rhs[j] = ints[j];
-    h.solve_host(rhs.data(), true);
+    // A^T q = ints in reference order; in kernel order (rows rotated by rrot, cols by crot) the
+    // transposed system reads its right-hand side rotated by crot and returns q rotated by rrot.
+    long const nn = b.n;
+    std::vector<double> rk(nn), rhs(nn);
+    for (long j = 0; j < nn; ++j) rk[j] = ints[(j + b.crot) % nn];
+    h.solve_host(rk.data(), true);
+    for (long i = 0; i < nn; ++i) rhs[(i + b.rrot) % nn] = rk[i];
     long const nv = b.n - b.nbv_lo - b.nbv_hi;
     for (int i = 0; i < b.nbv_lo; ++i) qlo[i] = rhs[i] * ipow(b.dx, i + b.odd);
     for (long i = 0; i < nv; ++i) q[i] = rhs[b.nbv_lo + i];
