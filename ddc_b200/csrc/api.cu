@@ -83,13 +83,18 @@ Evaluator* create_evaluator(Basis const& basis, int ex_lo, int ex_hi)
         BasisDesc const& D = e->basis.desc;
         int const nk = int(e->basis.knots.size());
         int const d = D.degree;
+        auto const& t = e->basis.knots;
+        // knot pairs (t_i, t_i+1)
+        std::vector<double> kp(size_t(2) * (nk - 1));
+        for (int i = 0; i + 1 < nk; ++i) {
+            kp[2 * i] = t[i];
+            kp[2 * i + 1] = t[i + 1];
+        }
+        auto inv = [&](long a, long b) { return t[b] > t[a] ? 1.0 / (t[b] - t[a]) : 0.0; };
         // knot-span inverses 1/(t[i+len]-t[i]) for len = 1..d (0 where the span is empty)
-        std::vector<double> inv(size_t(d) * nk, 0.0);
+        std::vector<double> ispan(size_t(d) * nk, 0.0);
         for (int len = 1; len <= d; ++len)
-            for (int i = 0; i + len < nk; ++i) {
-                double const s = e->basis.knots[i + len] - e->basis.knots[i];
-                inv[size_t(len - 1) * nk + i] = s > 0.0 ? 1.0 / s : 0.0;
-            }
+            for (int i = 0; i + len < nk; ++i) ispan[size_t(len - 1) * nk + i] = inv(i, i + len);
         // bucket table: the cell (knot index) holding the start of each of ncells uniform buckets
         int const nb = std::max(1, D.ncells);
         std::vector<int> lut(nb);
@@ -97,7 +102,7 @@ Evaluator* create_evaluator(Basis const& basis, int ex_lo, int ex_hi)
         int c = d;
         for (int bk = 0; bk < nb; ++bk) {
             double const x0 = D.rmin + double(bk) / scale;
-            while (c < d + D.ncells - 1 && x0 >= e->basis.knots[c + 1]) ++c;
+            while (c < d + D.ncells - 1 && x0 >= t[c + 1]) ++c;
             lut[bk] = c;
         }
         e->integrals.resize(e->basis.size());
@@ -106,18 +111,22 @@ Evaluator* create_evaluator(Basis const& basis, int ex_lo, int ex_hi)
         DDCB_CUDA_CHECK(cudaGetDevice(&dev));
         e->device = dev;
         upload_basis(e->basis, dev);
-        size_t const b_inv = inv.size() * 8, b_lut = lut.size() * 4, b_int = e->integrals.size() * 8;
-        size_t const o_lut = (b_inv + 255) / 256 * 256, o_int = o_lut + (b_lut + 255) / 256 * 256;
+        auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+        size_t const b_kp = kp.size() * 8, b_lut = lut.size() * 4, b_int = e->integrals.size() * 8;
+        size_t const b_isp = ispan.size() * 8;
+        size_t const o_lut = up(b_kp), o_isp = o_lut + up(b_lut), o_int = o_isp + up(b_isp);
         size_t const total = o_int + b_int + 8;
         DDCB_CUDA_CHECK(cudaMalloc(&e->d_block, total));
         char* base = static_cast<char*>(e->d_block);
-        DDCB_CUDA_CHECK(cudaMemcpy(base, inv.data(), b_inv, cudaMemcpyHostToDevice));
+        DDCB_CUDA_CHECK(cudaMemcpy(base, kp.data(), b_kp, cudaMemcpyHostToDevice));
         DDCB_CUDA_CHECK(cudaMemcpy(base + o_lut, lut.data(), b_lut, cudaMemcpyHostToDevice));
+        DDCB_CUDA_CHECK(cudaMemcpy(base + o_isp, ispan.data(), b_isp, cudaMemcpyHostToDevice));
         DDCB_CUDA_CHECK(cudaMemcpy(base + o_int, e->integrals.data(), b_int, cudaMemcpyHostToDevice));
         e->d_integrals = reinterpret_cast<double*>(base + o_int);
         e->eb.b = e->basis.device_desc();
-        e->eb.inv_span = reinterpret_cast<double const*>(base);
+        e->eb.kpairs = reinterpret_cast<double2 const*>(base);
         e->eb.lut = reinterpret_cast<int const*>(base + o_lut);
+        e->eb.inv_span = reinterpret_cast<double const*>(base + o_isp);
         e->eb.nbucket = nb;
         e->eb.bucket_scale = scale;
         e->eb.nk = nk;

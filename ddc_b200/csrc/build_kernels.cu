@@ -12,7 +12,7 @@ namespace {
 template <int TL, int KL, int KU>
 __global__ void __launch_bounds__(1024) build_kernel(const __grid_constant__ BuildArgs args)
 {
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) double smem[];
     solve_tile<TL, KL, KU>(args, smem);
     store_tile<TL>(args, smem);
 }

@@ -1,4 +1,10 @@
 // eval_device.cuh -- device-side point evaluation of a spline from a coefficient tile.
+//
+// Uniform bases need no tables: the cell comes from a scaled offset and the basis from the
+// uniform Cox-de Boor triangle. Non-uniform bases read the knots around the cell as (t_i, t_i+1)
+// pairs from shared memory (16-byte loads) and the knot-span inverses the Cox-de Boor triangle and
+// the derivative differences need from a small table built with the evaluator (L1-resident), so
+// the device evaluation divides nothing.
 #pragma once
 
 #include "bspline_math.cuh"
@@ -8,8 +14,9 @@ namespace ddcb {
 // Everything the kernels need to locate a point and evaluate the basis.
 struct EvalBasis
 {
-    BasisDesc b;              // b.knots: device knots (or a shared-memory copy inside a kernel)
-    const double* inv_span;   // degree x nk: inv_span[(len-1)*nk + i] = 1/(t[i+len]-t[i]) (0 if empty)
+    BasisDesc b;              // b.knots: device knots
+    const double2* kpairs;    // nk-1 pairs (t_i, t_i+1): device copy, or shared-memory copy in a kernel
+    const double* inv_span;   // degree x nk: inv_span[(len-1)*nk + i] = 1/(t[i+len] - t[i]) (0 if empty)
     const int* lut;           // nbucket entries: knot index of the cell holding each bucket start
     int nbucket;
     double bucket_scale;      // nbucket / (rmax - rmin)
@@ -64,14 +71,48 @@ __device__ __forceinline__ int nonuniform_locate(EvalBasis const& eb, double x)
     int bk = static_cast<int>((x - eb.b.rmin) * eb.bucket_scale);
     bk = bk < 0 ? 0 : (bk >= eb.nbucket ? eb.nbucket - 1 : bk);
     int c = __ldg(eb.lut + bk);
-    double const* K = eb.b.knots;
-    while (c < last && x >= K[c + 1]) ++c;
-    while (c > d && x < K[c]) --c;
+    double2 p = eb.kpairs[c];
+    while (c < last && x >= p.y) p = eb.kpairs[++c];
+    while (c > d && x < p.x) p = eb.kpairs[--c];
     return c;
 }
 
-// s(x) without boundary handling (spline_evaluator.hpp:556-605). C[i*cs] is the coefficient of
-// B-spline i.
+// The 2P knots t[c-P+1 .. c+P] around cell c (P >= 1), by P pair loads.
+template <int P>
+__device__ __forceinline__ void load_knots(EvalBasis const& eb, int c, double* kn)
+{
+#pragma unroll
+    for (int q = 0; q < P; ++q) {
+        double2 const p = eb.kpairs[c - P + 1 + 2 * q];
+        kn[2 * q] = p.x;
+        kn[2 * q + 1] = p.y;
+    }
+}
+
+// Non-uniform Cox-de Boor values of degree P on cell c (bsplines_non_uniform.hpp:459-497), with
+// the knot-span inverses read from the span table (ispan = inv_span + c: entry (j, r) is
+// 1/(t[c+r+1] - t[c+r-j]) at ispan[j*nk + r - j]).
+template <int P>
+__device__ __forceinline__ void nonuniform_values_span(const double* kn, const double* ispan, int nk, double x, double* v)
+{
+    double left[P + 1], right[P + 1];
+    v[0] = 1.0;
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+        left[j] = x - kn[P - 1 - j];  // x - t[c-j]
+        right[j] = kn[P + j] - x;     // t[c+j+1] - x
+        double saved = 0.0;
+#pragma unroll
+        for (int r = 0; r < j + 1; ++r) {
+            double const temp = v[r] * __ldg(ispan + j * nk + r - j);
+            v[r] = saved + right[r] * temp;
+            saved = left[j - r] * temp;
+        }
+        v[j + 1] = saved;
+    }
+}
+
+// s(x) without boundary handling (spline_evaluator.hpp:556-605).
 template <int D, bool UNI, class Acc>
 __device__ __forceinline__ double eval_value_no_bc(EvalBasis const& eb, double x, Acc const& C)
 {
@@ -83,8 +124,10 @@ __device__ __forceinline__ double eval_value_no_bc(EvalBasis const& eb, double x
         uniform_values_t<D>(off, v);
     } else {
         int const ck = nonuniform_locate(eb, x);
-        nonuniform_values_t<D>(eb.b.knots, eb.inv_span, eb.nk, ck, x, v);
         jmin = ck - D;
+        double kn[2 * D];
+        load_knots<D>(eb, ck, kn);
+        nonuniform_values_span<D>(kn, eb.inv_span + ck, eb.nk, x, v);
     }
     int const r0 = C.row0(jmin);
     double y = 0.0;
@@ -114,7 +157,8 @@ __device__ __forceinline__ double eval_value_bc(EvalBasis const& eb, int ex_lo, 
 }
 
 // d^ORDER s / dx^ORDER at x (spline_evaluator.hpp:388-430, no boundary handling): ORDER rounds of
-// divided differences of the d+1 coefficients of the cell, then the degree-(D-ORDER) basis.
+// divided differences of the D+1 coefficients of the cell (the derivative spline, de Boor,
+// "A Practical Guide to Splines", X.(15)), then the degree-(D-ORDER) basis.
 template <int D, int ORDER, bool UNI, class Acc>
 __device__ __forceinline__ double eval_deriv_no_bc(EvalBasis const& eb, double x, Acc const& C)
 {
@@ -128,10 +172,16 @@ __device__ __forceinline__ double eval_deriv_no_bc(EvalBasis const& eb, double x
         uniform_values_t<P>(off, v);
     } else {
         int const ck = nonuniform_locate(eb, x);
-        nonuniform_values_t<P>(eb.b.knots, eb.inv_span, eb.nk, ck, x, v);
         jmin = ck - D;
+        if constexpr (P > 0) {
+            double kn[2 * P];
+            load_knots<P>(eb, ck, kn);
+            nonuniform_values_span<P>(kn, eb.inv_span + ck, eb.nk, x, v);
+        } else {
+            v[0] = 1.0;
+        }
     }
-    const double* ispan = eb.inv_span + jmin; // knot-span inverses starting at knot jmin
+    const double* dspan = eb.inv_span + jmin; // 1/(t[jmin+i+len] - t[jmin+i]) at dspan[(len-1)*nk + i]
     int const r0 = C.row0(jmin);
 #pragma unroll
     for (int i = 0; i < D + 1; ++i) cc[i] = C.get(r0, i);
@@ -139,12 +189,8 @@ __device__ __forceinline__ double eval_deriv_no_bc(EvalBasis const& eb, double x
     for (int k = 1; k <= ORDER; ++k) {
 #pragma unroll
         for (int i = D; i >= k; --i) {
-            if (UNI) {
-                cc[i] = (cc[i] - cc[i - 1]) * eb.b.inv_step;
-            } else {
-                // c^(k)_j = (D-k+1) (c_j - c_{j-1}) / (t_{j+D-k+1} - t_j), j = jmin + i
-                cc[i] = double(D - k + 1) * (cc[i] - cc[i - 1]) * __ldg(ispan + (D - k) * eb.nk + i);
-            }
+            if (UNI) cc[i] = (cc[i] - cc[i - 1]) * eb.b.inv_step;
+            else cc[i] = double(D - k + 1) * (cc[i] - cc[i - 1]) * __ldg(dspan + (D - k) * eb.nk + i);
         }
     }
     double y = 0.0;

@@ -44,12 +44,18 @@ __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src)
 
 constexpr int kEvalThreads = 512;
 
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
+{
+    unsigned const s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+
 template <int D, int TLE, int ORDER, bool UNI>
 __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const __grid_constant__ EvalArgs a)
 {
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) double smem[];
     double* C = smem;                                  // size x TLE coefficient tile
-    double* K = C + (size_t)a.size * TLE;              // knots (non-uniform)
+    double2* K = reinterpret_cast<double2*>(C + (size_t)a.size * TLE); // knot pairs (non-uniform)
     int const tid = threadIdx.x;
     int const l = tid % TLE;
     int const c = tid / TLE;
@@ -61,12 +67,12 @@ __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const __grid_constan
         for (int r = c; r < a.size; r += nct) cp_async8(C + r * TLE + l, a.coefs + r * a.lc.stride + oc);
     }
     if (!UNI)
-        for (int i = tid; i < a.eb.nk; i += blockDim.x) cp_async8(K + i, a.eb.b.knots + i);
+        for (int i = tid; i < a.eb.nk - 1; i += blockDim.x) cp_async16(K + i, a.eb.kpairs + i);
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
     if (!live) return;
     EvalBasis eb = a.eb;
-    if (!UNI) eb.b.knots = K;
+    if (!UNI) eb.kpairs = K;
     int64_t const ox = line_offset(a.lx, line);
     int64_t const oo = line_offset(a.lo, line);
     int64_t const m = a.lx.n;
@@ -155,7 +161,7 @@ void launch_eval(Evaluator const& e, int order, double* out, Lines const& lo, do
     a.lo = lo;
     if (a.nlines == 0 || lx.n == 0) return;
     constexpr int TLE = 8;
-    size_t sm = sizeof(double) * ((size_t)a.size * TLE + (e.eb.b.uniform ? 0 : (size_t)e.eb.nk));
+    size_t sm = sizeof(double) * ((size_t)a.size * TLE + (e.eb.b.uniform ? 0 : 2 * (size_t)e.eb.nk));
     launch_deg<TLE>(a, order, sm, s);
 }
 

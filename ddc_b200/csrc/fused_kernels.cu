@@ -27,10 +27,11 @@ template <int TL, int KL, int KU, int D, int ORDER, bool UNI>
 __global__ void __launch_bounds__(1024) build_eval_kernel(const __grid_constant__ BuildArgs args,
                                                           const __grid_constant__ FusedEval fe)
 {
-    extern __shared__ double smem[];
-    double* K = smem + tile_doubles(args.t, TL, KL, KU); // knots (non-uniform)
+    extern __shared__ __align__(16) double smem[];
+    // knot pairs (non-uniform) after the tile, at an even double offset (16-byte aligned)
+    double2* K = reinterpret_cast<double2*>(smem + ((tile_doubles(args.t, TL, KL, KU) + 1) & ~size_t(1)));
     if (!UNI)
-        for (int i = threadIdx.x; i < fe.eb.nk; i += blockDim.x) K[i] = fe.eb.b.knots[i];
+        for (int i = threadIdx.x; i < fe.eb.nk - 1; i += blockDim.x) K[i] = fe.eb.kpairs[i];
     solve_tile<TL, KL, KU>(args, smem);
     store_tile<TL>(args, smem);
     int const tid = threadIdx.x;
@@ -40,7 +41,7 @@ __global__ void __launch_bounds__(1024) build_eval_kernel(const __grid_constant_
     int64_t const line = (int64_t)blockIdx.x * TL + l;
     if (line >= args.nlines) return;
     EvalBasis eb = fe.eb;
-    if (!UNI) eb.b.knots = K;
+    if (!UNI) eb.kpairs = K;
     int64_t const ox = line_offset(fe.lx, line);
     int64_t const oo = line_offset(fe.lo, line);
     int64_t const m = fe.lx.n;
@@ -64,7 +65,7 @@ template <int KL, int KU, int D, int ORDER, bool UNI>
 bool launch5(BuildArgs const& args, FusedEval const& fe, cudaStream_t s)
 {
     constexpr int TL = 8;
-    size_t const sm = sizeof(double) * (tile_doubles(args.t, TL, KL, KU) + (UNI ? 0 : (size_t)fe.eb.nk));
+    size_t const sm = sizeof(double) * (tile_doubles(args.t, TL, KL, KU) + (UNI ? 0 : 2 * (size_t)fe.eb.nk + 2));
     int dev = 0, optin = 0;
     DDCB_CUDA_CHECK(cudaGetDevice(&dev));
     DDCB_CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
