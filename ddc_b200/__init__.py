@@ -5,11 +5,13 @@ of include/ddcb.h; this package is the host-side mirror of the reference's splin
 """
 from . import _lib
 from ._lib import DdcbError
-from .splines import (BSplines, Extrapolation, NonUniformBSplines, SplineBuilder, SplineBuilderClosure,
-                      SplineEvaluator, UniformBSplines, greville_points, lines_of, n_boundary_equations)
+from .splines import (BSplines, Extrapolation, NonUniformBSplines, SplineBuilder, SplineBuilder2D, SplineBuilderClosure,
+                      SplineEvaluator, SplineEvaluator2D, UniformBSplines, greville_points, lines_of,
+                      n_boundary_equations)
 
 __all__ = [
-    "BSplines", "UniformBSplines", "NonUniformBSplines", "SplineBuilder", "SplineEvaluator", "SplineBuilderClosure",
+    "BSplines", "UniformBSplines", "NonUniformBSplines", "SplineBuilder", "SplineEvaluator", "SplineBuilder2D",
+    "SplineEvaluator2D", "SplineBuilderClosure",
     "Extrapolation", "greville_points", "lines_of", "n_boundary_equations", "DdcbError", "load_library",
 ]
 

@@ -83,6 +83,10 @@ SIGNATURES = {
     "ddcb_eval": [_vp, _vp, Lines, _vp, Lines, _vp, Lines, _vp],
     "ddcb_eval_deriv": [_vp, C.c_int32, _vp, Lines, _vp, Lines, _vp, Lines, _vp],
     "ddcb_integrate": [_vp, _vp, C.c_int64, _vp, Lines, _vp],
+    "ddcb_build2d_workspace_bytes": [_vp, _vp, C.c_int64, C.POINTER(C.c_uint64)],
+    "ddcb_build2d": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int64, _vp, C.c_uint64, _vp],
+    "ddcb_eval2d": [_vp, _vp, C.c_int32, C.c_int32, _vp, _vp, _vp, C.c_int64, C.c_int64, _vp],
+    "ddcb_integrate2d": [_vp, _vp, _vp, _vp, C.c_int64, _vp],
     "ddcb_build_eval": [_vp, _vp, C.c_int32, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines,
                         C.POINTER(C.c_int32), _vp],
 }

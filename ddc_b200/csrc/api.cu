@@ -475,4 +475,87 @@ ddcb_status ddcb_integrate(ddcb_evaluator h, double* out, int64_t out_outer_stri
     });
 }
 
+ddcb_status ddcb_build2d_workspace_bytes(ddcb_builder b1, ddcb_builder b2, int64_t nbatch, uint64_t* bytes)
+{
+    return guarded([&] {
+        require(b1 && b2 && bytes, "NULL argument");
+        require(nbatch >= 0, "negative batch");
+        *bytes = nbatch ? ddcb::build2d_workspace_bytes(*b1->b, *b2->b, nbatch) : 0;
+    });
+}
+
+ddcb_status ddcb_build2d(ddcb_builder h1, ddcb_builder h2, double* coefs, const double* vals, const double* dmin1,
+                         const double* dmax1, const double* dmin2, const double* dmax2, const double* m11,
+                         const double* m21, const double* m12, const double* m22, int64_t nbatch, void* workspace,
+                         uint64_t workspace_bytes, ddcb_stream stream)
+{
+    return guarded([&] {
+        require(h1 && h2, "builder is NULL");
+        require(nbatch >= 0, "negative batch");
+        if (nbatch == 0) return;
+        ddcb::Builder const& b1 = *h1->b;
+        ddcb::Builder const& b2 = *h2->b;
+        require(coefs && vals, "coefs/vals pointer is NULL");
+        bool const h1lo = b1.lo == DDCB_HERMITE && b1.nbv_lo > 0, h1hi = b1.hi == DDCB_HERMITE && b1.nbv_hi > 0;
+        bool const h2lo = b2.lo == DDCB_HERMITE && b2.nbv_lo > 0, h2hi = b2.hi == DDCB_HERMITE && b2.nbv_hi > 0;
+        require(!h1lo || dmin1, "derivs_min1 is required by the lower HERMITE closure of dimension 1");
+        require(!h1hi || dmax1, "derivs_max1 is required by the upper HERMITE closure of dimension 1");
+        require(!h2lo || dmin2, "derivs_min2 is required by the lower HERMITE closure of dimension 2");
+        require(!h2hi || dmax2, "derivs_max2 is required by the upper HERMITE closure of dimension 2");
+        require(!(h1lo && h2lo) || m11, "mixed_derivs_min1_min2 is required");
+        require(!(h1hi && h2lo) || m21, "mixed_derivs_max1_min2 is required");
+        require(!(h1lo && h2hi) || m12, "mixed_derivs_min1_max2 is required");
+        require(!(h1hi && h2hi) || m22, "mixed_derivs_max1_max2 is required");
+        int dev = 0;
+        DDCB_CUDA_CHECK(cudaGetDevice(&dev));
+        require(dev == b1.device && dev == b2.device, "the builders were created for another device");
+        size_t const need = ddcb::build2d_workspace_bytes(b1, b2, nbatch);
+        cudaStream_t const s = reinterpret_cast<cudaStream_t>(stream);
+        void* ws = workspace;
+        bool owned = false;
+        if (ws == nullptr) {
+            DDCB_CUDA_CHECK(cudaMallocAsync(&ws, need, s));
+            owned = true;
+        } else {
+            require(workspace_bytes >= need, "workspace too small (see ddcb_build2d_workspace_bytes)");
+        }
+        try {
+            ddcb::launch_build2d(b1, b2, coefs, vals, h1lo ? dmin1 : nullptr, h1hi ? dmax1 : nullptr, h2lo ? dmin2 : nullptr,
+                                 h2hi ? dmax2 : nullptr, (h1lo && h2lo) ? m11 : nullptr, (h1hi && h2lo) ? m21 : nullptr,
+                                 (h1lo && h2hi) ? m12 : nullptr, (h1hi && h2hi) ? m22 : nullptr, nbatch,
+                                 static_cast<double*>(ws), s);
+        } catch (...) {
+            if (owned) cudaFreeAsync(ws, s);
+            throw;
+        }
+        if (owned) DDCB_CUDA_CHECK(cudaFreeAsync(ws, s));
+    });
+}
+
+ddcb_status ddcb_eval2d(ddcb_evaluator h1, ddcb_evaluator h2, int32_t o1, int32_t o2, double* out, const double* coords,
+                        const double* coefs, int64_t npoints, int64_t nbatch, ddcb_stream stream)
+{
+    return guarded([&] {
+        require(h1 && h2, "evaluator is NULL");
+        require(npoints >= 0 && nbatch >= 0, "negative size");
+        require(o1 >= 0 && o1 <= 1 && o2 >= 0 && o2 <= 1, "2D derivative orders must be 0 or 1");
+        if (npoints == 0 || nbatch == 0) return;
+        require(out && coords && coefs, "NULL data pointer");
+        require((reinterpret_cast<uintptr_t>(coords) & 15) == 0, "coords must be 16-byte aligned (coordinate pairs)");
+        ddcb::launch_eval2d(*h1->e, *h2->e, o1, o2, out, coords, coefs, npoints, nbatch, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+ddcb_status ddcb_integrate2d(ddcb_evaluator h1, ddcb_evaluator h2, double* out, const double* coefs, int64_t nbatch,
+                             ddcb_stream stream)
+{
+    return guarded([&] {
+        require(h1 && h2, "evaluator is NULL");
+        require(nbatch >= 0, "negative batch");
+        if (nbatch == 0) return;
+        require(out && coefs, "NULL data pointer");
+        ddcb::launch_integrate2d(*h1->e, *h2->e, out, coefs, nbatch, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
 } // extern "C"

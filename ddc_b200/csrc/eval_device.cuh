@@ -210,3 +210,68 @@ __device__ __forceinline__ double eval_point(EvalBasis const& eb, int ex_lo, int
 #endif // __CUDACC__
 
 } // namespace ddcb
+
+namespace ddcb {
+
+#if defined(__CUDACC__)
+
+// Values of the ORDER-th derivative of the D+1 non-zero degree-D B-splines at x (the quantity the
+// reference takes from eval_basis_and_n_derivs, bsplines_*.hpp); returns the first B-spline index.
+// The degree-(D-ORDER) basis is raised back to degree D with the transpose of the derivative
+// differencing: d/dx B_{i,p} = p/(t_{i+p}-t_i) B_{i,p-1} - p/(t_{i+p+1}-t_{i+1}) B_{i+1,p-1}.
+template <int D, int ORDER, bool UNI>
+__device__ __forceinline__ int basis_derivs(EvalBasis const& eb, double x, double* val)
+{
+    constexpr int P = D - ORDER;
+    double w[D + 2];
+    int jmin;
+    if (UNI) {
+        double off;
+        jmin = uniform_cell(eb.b, x, off);
+        uniform_values_t<P>(off, w + ORDER);
+    } else {
+        int const ck = nonuniform_locate(eb, x);
+        jmin = ck - D;
+        if constexpr (P > 0) {
+            double kn[2 * P];
+            load_knots<P>(eb, ck, kn);
+            nonuniform_values_span<P>(kn, eb.inv_span + ck, eb.nk, x, w + ORDER);
+        } else {
+            w[ORDER] = 1.0;
+        }
+    }
+    // w[i] holds the value for B-spline jmin + i of the current degree, for i in [k, D]
+#pragma unroll
+    for (int k = ORDER; k >= 1; --k) {
+        // degree p = D-k+1 from degree D-k: entries i in [k-1, D]
+        int constexpr dummy = 0;
+        (void)dummy;
+        double nw[D + 2];
+#pragma unroll
+        for (int i = 0; i <= D; ++i) nw[i] = 0.0;
+#pragma unroll
+        for (int i = k - 1; i <= D; ++i) {
+            double const a = (i >= k) ? w[i] : 0.0;       // B_{i, p-1}
+            double const b = (i + 1 <= D) ? w[i + 1] : 0.0; // B_{i+1, p-1}
+            double fa, fb;
+            if (UNI) {
+                fa = eb.b.inv_step;
+                fb = eb.b.inv_step;
+            } else {
+                int const p = D - k + 1;
+                fa = double(p) * __ldg(eb.inv_span + (p - 1) * eb.nk + jmin + i);
+                fb = double(p) * __ldg(eb.inv_span + (p - 1) * eb.nk + jmin + i + 1);
+            }
+            nw[i] = fa * a - fb * ((i + 1 <= D && i + 1 >= k) ? b : 0.0);
+        }
+#pragma unroll
+        for (int i = 0; i <= D; ++i) w[i] = nw[i];
+    }
+#pragma unroll
+    for (int i = 0; i <= D; ++i) val[i] = w[i];
+    return jmin;
+}
+
+#endif
+
+} // namespace ddcb

@@ -1,0 +1,255 @@
+// tensor2d.cu -- tensor-product 2D builder and evaluator (SplineBuilder2D, SplineEvaluator2D;
+// spline_builder_2d.hpp:526-651, spline_evaluator_2d.hpp:342-826) for the layout
+// (x1, x2, batch) with the batch contiguous.
+//
+// Builder: the reference's four 1D passes (dim-2 derivative slabs and values along x1, then the
+// x2 pass over the result), run by the 1D build kernel with strided line descriptors. The batch is
+// processed in groups of fields whose x1-pass result fits comfortably in L2, so the x2 pass reads
+// it back from L2 rather than HBM; the workspace holds one group.
+// Evaluator: a warp handles 32 fields of one point, so each of the (d1+1)(d2+1) coefficient
+// gathers is one coalesced 256-byte load, and consecutive points of a block share coefficients
+// through L1.
+#include <algorithm>
+
+#include "build_device.cuh"
+#include "eval_device.cuh"
+
+namespace ddcb {
+
+namespace {
+
+int64_t group_fields(Builder const& b1, Builder const& b2, int64_t nbatch)
+{
+    int64_t const per_field = b1.basis.size() * int64_t(b2.points.size() + b2.nbv_lo + b2.nbv_hi) * 8;
+    int64_t g = std::max<int64_t>(1, (int64_t(40) << 20) / std::max<int64_t>(per_field, 1));
+    return std::min(g, nbatch);
+}
+
+} // namespace
+
+size_t build2d_workspace_bytes(Builder const& b1, Builder const& b2, int64_t nbatch)
+{
+    int64_t const G = group_fields(b1, b2, nbatch);
+    return size_t(b1.basis.size()) * size_t(b2.points.size() + b2.nbv_lo + b2.nbv_hi) * size_t(G) * 8;
+}
+
+void launch_build2d(Builder const& b1, Builder const& b2, double* coefs, double const* vals, double const* dmin1,
+                    double const* dmax1, double const* dmin2, double const* dmax2, double const* m11, double const* m21,
+                    double const* m12, double const* m22, int64_t B, double* ws, cudaStream_t s)
+{
+    int64_t const np1 = int64_t(b1.points.size()), np2 = int64_t(b2.points.size());
+    int64_t const s1 = b1.basis.size(), s2 = b2.basis.size();
+    int64_t const nlo1 = b1.nbv_lo, nhi1 = b1.nbv_hi, nlo2 = b2.nbv_lo, nhi2 = b2.nbv_hi;
+    bool const her_lo2 = b2.lo == DDCB_HERMITE && nlo2 > 0, her_hi2 = b2.hi == DDCB_HERMITE && nhi2 > 0;
+    int64_t const G0 = group_fields(b1, b2, B);
+    Lines const none {0, 1, 0, 0, 0};
+    for (int64_t f0 = 0; f0 < B; f0 += G0) {
+        int64_t const G = std::min(G0, B - f0);
+        double* S1 = ws;                       // (s1, np2, G)
+        double* S1lo = S1 + s1 * np2 * G;      // (s1, nlo2, G)
+        double* S1hi = S1lo + s1 * nlo2 * G;   // (s1, nhi2, G)
+        // lines of an x1 pass over an (x1, q, B) array restricted to the group: (q, field)
+        auto x1_lines = [&](int64_t n, int64_t nq, int64_t ld) { return Lines {n, nq * ld, G, nq, ld}; };
+        // (a) x1 pass over the lower dim-2 derivative slab, with the mixed derivatives as Hermite data
+        if (her_lo2) {
+            launch_build(b1, S1lo, x1_lines(s1, nlo2, G), dmin2 + f0, x1_lines(np1, nlo2, B), m11 ? m11 + f0 : nullptr,
+                               m11 ? x1_lines(nlo1, nlo2, B) : none, m21 ? m21 + f0 : nullptr,
+                               m21 ? x1_lines(nhi1, nlo2, B) : none, s);
+        }
+        // (b) x1 pass over the values
+        launch_build(b1, S1, x1_lines(s1, np2, G), vals + f0, x1_lines(np1, np2, B), dmin1 ? dmin1 + f0 : nullptr,
+                           dmin1 ? x1_lines(nlo1, np2, B) : none, dmax1 ? dmax1 + f0 : nullptr,
+                           dmax1 ? x1_lines(nhi1, np2, B) : none, s);
+        // (c) x1 pass over the upper dim-2 derivative slab
+        if (her_hi2) {
+            launch_build(b1, S1hi, x1_lines(s1, nhi2, G), dmax2 + f0, x1_lines(np1, nhi2, B), m12 ? m12 + f0 : nullptr,
+                               m12 ? x1_lines(nlo1, nhi2, B) : none, m22 ? m22 + f0 : nullptr,
+                               m22 ? x1_lines(nhi1, nhi2, B) : none, s);
+        }
+        // (d) x2 pass: lines (row r of the x1 coefficients, field) of the x1 results
+        Lines const lv2 {np2, G, G, s1, np2 * G};
+        Lines const llo2 {nlo2, G, G, s1, nlo2 * G};
+        Lines const lhi2 {nhi2, G, G, s1, nhi2 * G};
+        Lines const lc2 {s2, B, G, s1, s2 * B};
+        launch_build(b2, coefs + f0, lc2, S1, lv2, her_lo2 ? S1lo : nullptr, her_lo2 ? llo2 : none,
+                           her_hi2 ? S1hi : nullptr, her_hi2 ? lhi2 : none, s);
+    }
+}
+
+namespace {
+
+struct Eval2dArgs
+{
+    EvalBasis e1, e2;
+    int ex1lo, ex1hi, ex2lo, ex2hi;
+    const double* coords; // (m, B) pairs (x1, x2)
+    const double* coefs;  // (size1, size2, B)
+    double* out;          // (m, B)
+    int64_t m, B, size2;
+};
+
+template <int D1, int D2, int O1, int O2, bool U1, bool U2>
+__device__ __forceinline__ double eval2d_point(Eval2dArgs const& a, double x1, double x2, const double* C)
+{
+    double v1[D1 + 1], v2[D2 + 1];
+    int const j1 = basis_derivs<D1, O1, U1>(a.e1, x1, v1);
+    int const j2 = basis_derivs<D2, O2, U2>(a.e2, x2, v2);
+    int64_t const B = a.B;
+    double y = 0.0;
+#pragma unroll
+    for (int i = 0; i < D1 + 1; ++i) {
+        const double* row = C + ((int64_t)(j1 + i) * a.size2 + j2) * B;
+        double t = 0.0;
+#pragma unroll
+        for (int j = 0; j < D2 + 1; ++j) t = fma(__ldg(row + j * B), v2[j], t);
+        y = fma(t, v1[i], y);
+    }
+    return y;
+}
+
+// Boundary handling of SplineEvaluator2D::eval (spline_evaluator_2d.hpp:680-727): periodic wraps,
+// then the extrapolation rules of the non-periodic dimensions (null: 0; constant: the value at the
+// domain end, the other coordinate clamped when that dimension is not periodic,
+// constant_extrapolation_rule.hpp:143-193).
+template <int D1, int D2, bool U1, bool U2>
+__device__ __forceinline__ double eval2d_bc(Eval2dArgs const& a, double x1, double x2, const double* C)
+{
+    BasisDesc const& b1 = a.e1.b;
+    BasisDesc const& b2 = a.e2.b;
+    if (b1.periodic) x1 = periodic_wrap(b1, x1);
+    if (b2.periodic) x2 = periodic_wrap(b2, x2);
+    auto clamp = [](double v, double lo, double hi) { return v < lo ? lo : (v > hi ? hi : v); };
+    if (!b1.periodic && (x1 < b1.rmin || x1 > b1.rmax)) {
+        bool const low = x1 < b1.rmin;
+        if ((low ? a.ex1lo : a.ex1hi) == 1) return 0.0;
+        x1 = low ? b1.rmin : b1.rmax;
+        if (!b2.periodic) x2 = clamp(x2, b2.rmin, b2.rmax);
+    } else if (!b2.periodic && (x2 < b2.rmin || x2 > b2.rmax)) {
+        bool const low = x2 < b2.rmin;
+        if ((low ? a.ex2lo : a.ex2hi) == 1) return 0.0;
+        x2 = low ? b2.rmin : b2.rmax;
+        if (!b1.periodic) x1 = clamp(x1, b1.rmin, b1.rmax);
+    }
+    return eval2d_point<D1, D2, 0, 0, U1, U2>(a, x1, x2, C);
+}
+
+constexpr int kPts2d = 8; // points (warps) per block; 32 fields per warp
+
+template <int D1, int D2, int O1, int O2, bool U1, bool U2>
+__global__ void __launch_bounds__(32 * kPts2d) eval2d_kernel(const __grid_constant__ Eval2dArgs a, int64_t pts_per_block)
+{
+    int const lane = threadIdx.x & 31;
+    int const w = threadIdx.x >> 5;
+    int64_t const b = (int64_t)blockIdx.y * 32 + lane;
+    if (b >= a.B) return;
+    int64_t const p0 = (int64_t)blockIdx.x * pts_per_block;
+    int64_t const p1 = min(p0 + pts_per_block, a.m);
+    const double* C = a.coefs + b;
+    for (int64_t p = p0 + w; p < p1; p += kPts2d) {
+        double2 const xy = reinterpret_cast<const double2*>(a.coords)[p * a.B + b];
+        double y;
+        if (O1 == 0 && O2 == 0) y = eval2d_bc<D1, D2, U1, U2>(a, xy.x, xy.y, C);
+        else y = eval2d_point<D1, D2, O1, O2, U1, U2>(a, xy.x, xy.y, C);
+        a.out[p * a.B + b] = y;
+    }
+}
+
+template <int D1, int D2, int O1, int O2>
+void launch_eval2d_u(Eval2dArgs const& a, cudaStream_t s)
+{
+    int64_t const ppb = 64;
+    dim3 grid((unsigned)((a.m + ppb - 1) / ppb), (unsigned)((a.B + 31) / 32));
+    bool const u1 = a.e1.b.uniform != 0, u2 = a.e2.b.uniform != 0;
+    if (u1 && u2) eval2d_kernel<D1, D2, O1, O2, true, true><<<grid, 32 * kPts2d, 0, s>>>(a, ppb);
+    else if (u1) eval2d_kernel<D1, D2, O1, O2, true, false><<<grid, 32 * kPts2d, 0, s>>>(a, ppb);
+    else if (u2) eval2d_kernel<D1, D2, O1, O2, false, true><<<grid, 32 * kPts2d, 0, s>>>(a, ppb);
+    else eval2d_kernel<D1, D2, O1, O2, false, false><<<grid, 32 * kPts2d, 0, s>>>(a, ppb);
+    DDCB_CUDA_CHECK(cudaGetLastError());
+}
+
+template <int D1, int D2>
+void launch_eval2d_o(Eval2dArgs const& a, int o1, int o2, cudaStream_t s)
+{
+    if (o1 == 0 && o2 == 0) launch_eval2d_u<D1, D2, 0, 0>(a, s);
+    else if (o1 == 1 && o2 == 0) launch_eval2d_u<D1, D2, 1, 0>(a, s);
+    else if (o1 == 0 && o2 == 1) launch_eval2d_u<D1, D2, 0, 1>(a, s);
+    else if (o1 == 1 && o2 == 1) launch_eval2d_u<D1, D2, 1, 1>(a, s);
+    else throw Error(DDCB_ERR_UNSUPPORTED, "2D derivative orders must be 0 or 1 in each dimension");
+}
+
+template <int D1>
+void launch_eval2d_d2(Eval2dArgs const& a, int o1, int o2, cudaStream_t s)
+{
+    switch (a.e2.b.degree) {
+    case 1: launch_eval2d_o<D1, 1>(a, o1, o2, s); break;
+    case 2: launch_eval2d_o<D1, 2>(a, o1, o2, s); break;
+    case 3: launch_eval2d_o<D1, 3>(a, o1, o2, s); break;
+    case 4: launch_eval2d_o<D1, 4>(a, o1, o2, s); break;
+    case 5: launch_eval2d_o<D1, 5>(a, o1, o2, s); break;
+    default: throw Error(DDCB_ERR_UNSUPPORTED, "degree must be in 1..5");
+    }
+}
+
+__global__ void integrate2d_kernel(const double* __restrict__ coefs, const double* __restrict__ i1, const double* __restrict__ i2,
+                                   int64_t s1, int64_t s2, int64_t B, double* __restrict__ out)
+{
+    // block: 32 fields x 32 row slots; each slot sums its rows, then a shared reduction
+    __shared__ double part[32][33];
+    int const lane = threadIdx.x & 31, slot = threadIdx.x >> 5;
+    int64_t const b = (int64_t)blockIdx.x * 32 + lane;
+    double acc = 0.0;
+    if (b < B)
+        for (int64_t r1 = slot; r1 < s1; r1 += 32) {
+            double t = 0.0;
+            const double* row = coefs + r1 * s2 * B + b;
+            for (int64_t r2 = 0; r2 < s2; ++r2) t = fma(row[r2 * B], __ldg(i2 + r2), t);
+            acc = fma(t, __ldg(i1 + r1), acc);
+        }
+    part[slot][lane] = acc;
+    __syncthreads();
+    if (slot == 0 && b < B) {
+        double s = 0.0;
+        for (int q = 0; q < 32; ++q) s += part[q][lane];
+        out[b] = s;
+    }
+}
+
+} // namespace
+
+void launch_eval2d(Evaluator const& e1, Evaluator const& e2, int o1, int o2, double* out, double const* coords,
+                   double const* coefs, int64_t m, int64_t B, cudaStream_t s)
+{
+    if (m == 0 || B == 0) return;
+    Eval2dArgs a {};
+    a.e1 = e1.eb;
+    a.e2 = e2.eb;
+    a.ex1lo = e1.ex_lo;
+    a.ex1hi = e1.ex_hi;
+    a.ex2lo = e2.ex_lo;
+    a.ex2hi = e2.ex_hi;
+    a.coords = coords;
+    a.coefs = coefs;
+    a.out = out;
+    a.m = m;
+    a.B = B;
+    a.size2 = e2.basis.size();
+    switch (e1.basis.desc.degree) {
+    case 1: launch_eval2d_d2<1>(a, o1, o2, s); break;
+    case 2: launch_eval2d_d2<2>(a, o1, o2, s); break;
+    case 3: launch_eval2d_d2<3>(a, o1, o2, s); break;
+    case 4: launch_eval2d_d2<4>(a, o1, o2, s); break;
+    case 5: launch_eval2d_d2<5>(a, o1, o2, s); break;
+    default: throw Error(DDCB_ERR_UNSUPPORTED, "degree must be in 1..5");
+    }
+}
+
+void launch_integrate2d(Evaluator const& e1, Evaluator const& e2, double* out, double const* coefs, int64_t B,
+                        cudaStream_t s)
+{
+    if (B == 0) return;
+    integrate2d_kernel<<<dim3((unsigned)((B + 31) / 32)), dim3(1024), 0, s>>>(coefs, e1.d_integrals, e2.d_integrals,
+                                                                            e1.basis.size(), e2.basis.size(), B, out);
+    DDCB_CUDA_CHECK(cudaGetLastError());
+}
+
+} // namespace ddcb

@@ -118,8 +118,9 @@ class BSplines:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            _lib.load().ddcb_bsplines_destroy(h)
+        L = getattr(_lib, "_lib", None) if _lib is not None else None
+        if h and L is not None:
+            L.ddcb_bsplines_destroy(h)
             self._h = None
 
     @property
@@ -188,8 +189,9 @@ class SplineBuilder:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            _lib.load().ddcb_builder_destroy(h)
+        L = getattr(_lib, "_lib", None) if _lib is not None else None
+        if h and L is not None:
+            L.ddcb_builder_destroy(h)
             self._h = None
 
     @property
@@ -261,8 +263,9 @@ class SplineEvaluator:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            _lib.load().ddcb_evaluator_destroy(h)
+        L = getattr(_lib, "_lib", None) if _lib is not None else None
+        if h and L is not None:
+            L.ddcb_evaluator_destroy(h)
             self._h = None
 
     def __call__(self, spline_eval, coords_eval, spline_coef, *, dim: int = 0, stream=None):
@@ -290,4 +293,82 @@ class SplineEvaluator:
         lc = lines_of(c, dim)
         assert out.numel() == lc.inner * lc.outer and out.is_contiguous()
         _lib.call("ddcb_integrate", self._h, _ptr(out), lc.inner, _ptr(c), lc, _stream_handle(stream))
+        return out
+
+
+class SplineBuilder2D:
+    """ddc::SplineBuilder2D: two 1D builders applied as the reference does (spline_builder_2d.hpp:526-651).
+
+    Data layout (x1, x2, batch...) with the batch contiguous: vals (np1, np2, *batch) ->
+    spline (size1, size2, *batch).
+    """
+
+    def __init__(self, builder1: SplineBuilder, builder2: SplineBuilder):
+        self.builder1, self.builder2 = builder1, builder2
+
+    def workspace_bytes(self, nbatch: int) -> int:
+        out = C.c_uint64()
+        _lib.call("ddcb_build2d_workspace_bytes", self.builder1._h, self.builder2._h, int(nbatch), C.byref(out))
+        return out.value
+
+    def __call__(self, spline, vals, derivs_min1=None, derivs_max1=None, derivs_min2=None, derivs_max2=None,
+                 mixed_derivs_min1_min2=None, mixed_derivs_max1_min2=None, mixed_derivs_min1_max2=None,
+                 mixed_derivs_max1_max2=None, *, workspace=None, stream=None):
+        spline = _dev_f64(spline, "spline")
+        vals = _dev_f64(vals, "vals")
+        assert spline.is_contiguous() and vals.is_contiguous()
+        nbatch = vals[0, 0].numel()
+        arrs = [derivs_min1, derivs_max1, derivs_min2, derivs_max2, mixed_derivs_min1_min2, mixed_derivs_max1_min2,
+                mixed_derivs_min1_max2, mixed_derivs_max1_max2]
+        arrs = [_dev_f64(a, "derivs") for a in arrs]
+        for a in arrs:
+            assert a is None or a.is_contiguous()
+        ws_ptr, ws_bytes = C.c_void_p(0), 0
+        if workspace is not None:
+            ws_ptr, ws_bytes = C.c_void_p(workspace.data_ptr()), workspace.numel() * workspace.element_size()
+        _lib.call("ddcb_build2d", self.builder1._h, self.builder2._h, _ptr(spline), _ptr(vals), *[_ptr(a) for a in arrs],
+                  int(nbatch), ws_ptr, ws_bytes, _stream_handle(stream))
+        return spline
+
+
+class SplineEvaluator2D:
+    """ddc::SplineEvaluator2D over two 1D evaluators (spline_evaluator_2d.hpp).
+
+    coords_eval: (*points, *batch, 2) coordinate pairs; spline_coef: (size1, size2, *batch).
+    """
+
+    def __init__(self, evaluator1: SplineEvaluator, evaluator2: SplineEvaluator):
+        self.evaluator1, self.evaluator2 = evaluator1, evaluator2
+
+    def _run(self, o1, o2, spline_eval, coords_eval, spline_coef, stream):
+        out = _dev_f64(spline_eval, "spline_eval")
+        x = _dev_f64(coords_eval, "coords_eval")
+        c = _dev_f64(spline_coef, "spline_coef")
+        assert out.is_contiguous() and x.is_contiguous() and c.is_contiguous()
+        nbatch = c[0, 0].numel()
+        npoints = out.numel() // max(nbatch, 1)
+        assert x.numel() == 2 * out.numel()
+        _lib.call("ddcb_eval2d", self.evaluator1._h, self.evaluator2._h, int(o1), int(o2), _ptr(out), _ptr(x), _ptr(c),
+                  int(npoints), int(nbatch), _stream_handle(stream))
+        return out
+
+    def __call__(self, spline_eval, coords_eval, spline_coef, *, stream=None):
+        return self._run(0, 0, spline_eval, coords_eval, spline_coef, stream)
+
+    def deriv_dim_1(self, spline_eval, coords_eval, spline_coef, *, stream=None):
+        return self._run(1, 0, spline_eval, coords_eval, spline_coef, stream)
+
+    def deriv_dim_2(self, spline_eval, coords_eval, spline_coef, *, stream=None):
+        return self._run(0, 1, spline_eval, coords_eval, spline_coef, stream)
+
+    def deriv_1_and_2(self, spline_eval, coords_eval, spline_coef, *, stream=None):
+        return self._run(1, 1, spline_eval, coords_eval, spline_coef, stream)
+
+    def integrate(self, integrals, spline_coef, *, stream=None):
+        out = _dev_f64(integrals, "integrals")
+        c = _dev_f64(spline_coef, "spline_coef")
+        nbatch = c[0, 0].numel()
+        assert out.numel() == nbatch and out.is_contiguous() and c.is_contiguous()
+        _lib.call("ddcb_integrate2d", self.evaluator1._h, self.evaluator2._h, _ptr(out), _ptr(c), int(nbatch),
+                  _stream_handle(stream))
         return out

@@ -66,3 +66,29 @@ def config2(B: int = 1 << 16, ncells: int = 1024, m: int = 1024, points=None):
         out["dhi"] = np.ascontiguousarray(np.stack([cos_family(1.0, k, ph, o) for o in (1, 2)]))
     out["coords"] = np.ascontiguousarray(splitmix_uniform(seed, 4, m * B).reshape(m, B))
     return out
+
+
+def config3(nfields: int = 64, ncells: int = 512):
+    """2D: x periodic cubic uniform (ncells) x y Hermite cubic uniform (ncells) on [0,1)x[0,1];
+    f = sin(2 pi x) cos(pi y) a_b + 0.01 N(0,1), evaluation at the semi-Lagrangian feet
+    (x - v dt, y), v ~ U[-1,1] per y row, dt = h/2. Arrays in (x, y, field) layout."""
+    seed = 0xDDC0 + 3
+    h = 1.0 / ncells
+    x = np.arange(ncells) * h                 # periodic cubic Greville points
+    y = np.arange(ncells + 1) * h             # Hermite cubic points (break points)
+    a = 0.5 + 1.5 * splitmix_uniform(seed, 1, nfields)
+    u1 = splitmix_uniform(seed, 2, ncells * (ncells + 1) * nfields)
+    u2 = splitmix_uniform(seed, 3, ncells * (ncells + 1) * nfields)
+    noise = (np.sqrt(-2.0 * np.log(np.maximum(u1, 1e-300))) * np.cos(2 * np.pi * u2)).reshape(ncells, ncells + 1, nfields)
+    base = np.sin(2 * np.pi * x)[:, None, None] * np.cos(np.pi * y)[None, :, None]
+    vals = base * a[None, None, :] + 0.01 * noise
+    # d/dy at y=0 and y=1 of the smooth part (the noise has no derivative): -pi sin(pi y) = 0 at both ends
+    dmin2 = np.zeros((ncells, 1, nfields))
+    dmax2 = np.zeros((ncells, 1, nfields))
+    v = 2.0 * splitmix_uniform(seed, 4, ncells + 1) - 1.0
+    dt = 0.5 * h
+    feet_x = x[:, None, None] - v[None, :, None] * dt + np.zeros((1, 1, nfields))
+    feet_y = y[None, :, None] + np.zeros((ncells, 1, nfields))
+    coords = np.ascontiguousarray(np.stack([feet_x, feet_y], axis=-1))
+    return dict(x=x, y=y, vals=np.ascontiguousarray(vals), dmin2=dmin2, dmax2=dmax2, coords=coords, ncells=ncells,
+                nfields=nfields)

@@ -167,6 +167,33 @@ ddcb_status ddcb_build_eval(ddcb_builder b, ddcb_evaluator e, int32_t order, dou
                             const double* coords, ddcb_lines coords_layout, double* out, ddcb_lines out_layout,
                             int32_t* fused, ddcb_stream stream);
 
+/* ---- 2D tensor product: SplineBuilder2D / SplineEvaluator2D on two 1D plans, for the layout
+ *      (x1, x2, batch) with the batch contiguous (the reference's layout_right of
+ *      DiscreteDomain<X1, X2, batch...>). ----------------------------------------------------- */
+/* Workspace of ddcb_build2d: the x1-pass result of one group of fields. */
+ddcb_status ddcb_build2d_workspace_bytes(ddcb_builder b1, ddcb_builder b2, int64_t nbatch, uint64_t* bytes);
+/* SplineBuilder2D::operator() (spline_builder_2d.hpp:455-651).
+ *   vals (np1, np2, nbatch) -> coefs (size1, size2, nbatch);
+ *   derivs_min1 / derivs_max1: (nbv1, np2, nbatch), read when b1's closure is HERMITE;
+ *   derivs_min2 / derivs_max2: (np1, nbv2, nbatch), read when b2's closure is HERMITE;
+ *   mixed_* (nbv1, nbv2, nbatch): cross derivatives at the four corners, read when both are HERMITE.
+ * workspace: ddcb_build2d_workspace_bytes bytes of device memory, or NULL to have the call
+ * allocate it stream-ordered (cudaMallocAsync / cudaFreeAsync on `stream`). */
+ddcb_status ddcb_build2d(ddcb_builder b1, ddcb_builder b2, double* coefs, const double* vals, const double* derivs_min1,
+                         const double* derivs_max1, const double* derivs_min2, const double* derivs_max2,
+                         const double* mixed_min1_min2, const double* mixed_max1_min2, const double* mixed_min1_max2,
+                         const double* mixed_max1_max2, int64_t nbatch, void* workspace, uint64_t workspace_bytes,
+                         ddcb_stream stream);
+/* SplineEvaluator2D::operator() (order1 = order2 = 0, with the periodic wraps / extrapolation rules)
+ * and deriv_dim_1 / deriv_dim_2 / deriv_1_and_2 (orders 0 or 1, no boundary handling)
+ * (spline_evaluator_2d.hpp:376-598): coords (npoints, nbatch) pairs (x1, x2) -> out (npoints, nbatch);
+ * coefs (size1, size2, nbatch). */
+ddcb_status ddcb_eval2d(ddcb_evaluator e1, ddcb_evaluator e2, int32_t order1, int32_t order2, double* out,
+                        const double* coords, const double* coefs, int64_t npoints, int64_t nbatch, ddcb_stream stream);
+/* SplineEvaluator2D::integrate (spline_evaluator_2d.hpp:616-660): out[b] = sum c(r1, r2, b) I1[r1] I2[r2]. */
+ddcb_status ddcb_integrate2d(ddcb_evaluator e1, ddcb_evaluator e2, double* out, const double* coefs, int64_t nbatch,
+                             ddcb_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -249,6 +249,7 @@ def build2d(b1: Builder, b2: Builder, vals, derivs_min1=None, derivs_max1=None, 
 
 def evaluate2d(bs1: BSplines, bs2: BSplines, c1, c2, coefs, orders=None,
                ex=(EX_NULL, EX_NULL, EX_NULL, EX_NULL), nthreads=None):
+    """orders None: value with boundary handling; else (o1, o2) derivative orders (eval_no_bc)."""
     """SplineEvaluator2D::operator() / deriv. c1, c2: (m, B) coordinates; coefs (size1, size2, B)."""
     c1 = np.ascontiguousarray(c1, dtype=np.float64)
     c2 = np.ascontiguousarray(c2, dtype=np.float64)
