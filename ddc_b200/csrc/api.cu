@@ -558,4 +558,38 @@ ddcb_status ddcb_integrate2d(ddcb_evaluator h1, ddcb_evaluator h2, double* out, 
     });
 }
 
+// No-allocation 2D build (see include/ddcb.h): identical validation to ddcb_build2d, scratch from
+// the library's static device array.
+ddcb_status ddcb_build2d_static_scratch(ddcb_builder h1, ddcb_builder h2, double* coefs, const double* vals,
+                                        const double* dmin1, const double* dmax1, const double* dmin2,
+                                        const double* dmax2, const double* m11, const double* m21, const double* m12,
+                                        const double* m22, int64_t nbatch, ddcb_stream stream)
+{
+    return guarded([&] {
+        require(h1 && h2, "builder is NULL");
+        require(nbatch >= 0, "negative batch");
+        if (nbatch == 0) return;
+        ddcb::Builder const& b1 = *h1->b;
+        ddcb::Builder const& b2 = *h2->b;
+        require(coefs && vals, "coefs/vals pointer is NULL");
+        bool const h1lo = b1.lo == DDCB_HERMITE && b1.nbv_lo > 0, h1hi = b1.hi == DDCB_HERMITE && b1.nbv_hi > 0;
+        bool const h2lo = b2.lo == DDCB_HERMITE && b2.nbv_lo > 0, h2hi = b2.hi == DDCB_HERMITE && b2.nbv_hi > 0;
+        require(!h1lo || dmin1, "derivs_min1 is required by the lower HERMITE closure of dimension 1");
+        require(!h1hi || dmax1, "derivs_max1 is required by the upper HERMITE closure of dimension 1");
+        require(!h2lo || dmin2, "derivs_min2 is required by the lower HERMITE closure of dimension 2");
+        require(!h2hi || dmax2, "derivs_max2 is required by the upper HERMITE closure of dimension 2");
+        require(!(h1lo && h2lo) || m11, "mixed_derivs_min1_min2 is required");
+        require(!(h1hi && h2lo) || m21, "mixed_derivs_max1_min2 is required");
+        require(!(h1lo && h2hi) || m12, "mixed_derivs_min1_max2 is required");
+        require(!(h1hi && h2hi) || m22, "mixed_derivs_max1_max2 is required");
+        int dev = 0;
+        DDCB_CUDA_CHECK(cudaGetDevice(&dev));
+        require(dev == b1.device && dev == b2.device, "the builders were created for another device");
+        ddcb::launch_build2d_static(b1, b2, coefs, vals, h1lo ? dmin1 : nullptr, h1hi ? dmax1 : nullptr,
+                                    h2lo ? dmin2 : nullptr, h2hi ? dmax2 : nullptr, (h1lo && h2lo) ? m11 : nullptr,
+                                    (h1hi && h2lo) ? m21 : nullptr, (h1lo && h2hi) ? m12 : nullptr,
+                                    (h1hi && h2hi) ? m22 : nullptr, nbatch, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
 } // extern "C"

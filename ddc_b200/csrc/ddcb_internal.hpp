@@ -174,6 +174,10 @@ void launch_build2d(Builder const& b1, Builder const& b2, double* coefs, double 
 void launch_eval2d(Evaluator const& e1, Evaluator const& e2, int o1, int o2, double* out, double const* coords,
                    double const* coefs, int64_t m, int64_t B, cudaStream_t s);
 void launch_integrate2d(Evaluator const& e1, Evaluator const& e2, double* out, double const* coefs, int64_t B, cudaStream_t s);
+size_t build2d_static_scratch_bytes();
+void launch_build2d_static(Builder const& b1, Builder const& b2, double* coefs, double const* vals, double const* dmin1,
+                           double const* dmax1, double const* dmin2, double const* dmax2, double const* m11,
+                           double const* m21, double const* m12, double const* m22, int64_t B, cudaStream_t s);
 
 // eval_kernels.cu
 void launch_eval(Evaluator const& e, int order, double* out, Lines const& lo, double const* coords, Lines const& lx,

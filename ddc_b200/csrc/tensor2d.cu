@@ -10,6 +10,8 @@
 // gathers is one coalesced 256-byte load, and consecutive points of a block share coefficients
 // through L1.
 #include <algorithm>
+#include <mutex>
+#include <string>
 
 #include "build_device.cuh"
 #include "eval_device.cuh"
@@ -250,6 +252,55 @@ void launch_integrate2d(Evaluator const& e1, Evaluator const& e2, double* out, d
     integrate2d_kernel<<<dim3((unsigned)((B + 31) / 32)), dim3(1024), 0, s>>>(coefs, e1.d_integrals, e2.d_integrals,
                                                                             e1.basis.size(), e2.basis.size(), B, out);
     DDCB_CUDA_CHECK(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------------------------
+// 2D build without any allocation: the x1-pass scratch lives in a fixed array of this library's
+// device image instead of caller or allocator memory.
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kStaticScratchBytes = size_t(48) << 20; // 48 MiB, held on every GPU that loads the library
+
+static __device__ __align__(256) double g_build2d_scratch[kStaticScratchBytes / sizeof(double)];
+
+std::mutex g_scratch_mutex;
+void* g_scratch_addr[256] = {};
+
+// Device address of the scratch array on the current device, looked up once per device. The host
+// symbol g_build2d_scratch is only a stand-in for the device array; kernels must be given the
+// address the runtime reports for the current device.
+double* static_scratch_for_current_device()
+{
+    int dev = 0;
+    DDCB_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) throw Error(DDCB_ERR_UNSUPPORTED, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (g_scratch_addr[dev] == nullptr) {
+        void* p = nullptr;
+        cudaError_t const e = cudaGetSymbolAddress(&p, g_build2d_scratch);
+        if (e != cudaSuccess || p == nullptr)
+            throw Error(DDCB_ERR_CUDA, std::string("cudaGetSymbolAddress of the static 2D scratch failed: ") + cudaGetErrorString(e));
+        g_scratch_addr[dev] = p;
+    }
+    return static_cast<double*>(g_scratch_addr[dev]);
+}
+
+} // namespace
+
+size_t build2d_static_scratch_bytes() { return kStaticScratchBytes; }
+
+void launch_build2d_static(Builder const& b1, Builder const& b2, double* coefs, double const* vals, double const* dmin1,
+                           double const* dmax1, double const* dmin2, double const* dmax2, double const* m11,
+                           double const* m21, double const* m12, double const* m22, int64_t B, cudaStream_t s)
+{
+    size_t const need = build2d_workspace_bytes(b1, b2, B);
+    if (need > kStaticScratchBytes)
+        throw Error(DDCB_ERR_UNSUPPORTED, "this 2D build needs " + std::to_string(need) + " bytes of scratch, more than the "
+                                              + std::to_string(kStaticScratchBytes)
+                                              + " bytes of the library's static scratch; use ddcb_build2d with a workspace");
+    double* ws = static_scratch_for_current_device();
+    launch_build2d(b1, b2, coefs, vals, dmin1, dmax1, dmin2, dmax2, m11, m21, m12, m22, B, ws, s);
 }
 
 } // namespace ddcb

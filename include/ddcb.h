@@ -184,6 +184,23 @@ ddcb_status ddcb_build2d(ddcb_builder b1, ddcb_builder b2, double* coefs, const 
                          const double* mixed_min1_min2, const double* mixed_max1_min2, const double* mixed_min1_max2,
                          const double* mixed_max1_max2, int64_t nbatch, void* workspace, uint64_t workspace_bytes,
                          ddcb_stream stream);
+/* 2D build that allocates nothing. No counterpart in the reference: this is an addition for callers
+ * that must not allocate device memory at call time -- code running where cudaMalloc is not
+ * allowed or not wanted (for instance inside a memory pool's budget, a real-time loop, or a host
+ * framework that owns all device memory), which also cannot hand over a workspace.
+ * Same arguments and results as ddcb_build2d with workspace == NULL, but the scratch of the x1 pass
+ * is a fixed array of 48 MiB (50331648 bytes) inside the library's device image, present on every
+ * GPU that loads the library until the process exits. Requests whose ddcb_build2d_workspace_bytes
+ * exceed it are rejected with DDCB_ERR_UNSUPPORTED. The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress, once per device); make that first call before
+ * any stream capture. All calls share the one array: calls whose work overlaps on the GPU (other
+ * streams, other host threads) race on it and must be ordered by the caller. The scratch needs no
+ * clearing: every value is written before it is read. */
+ddcb_status ddcb_build2d_static_scratch(ddcb_builder b1, ddcb_builder b2, double* coefs, const double* vals,
+                                        const double* derivs_min1, const double* derivs_max1, const double* derivs_min2,
+                                        const double* derivs_max2, const double* mixed_min1_min2,
+                                        const double* mixed_max1_min2, const double* mixed_min1_max2,
+                                        const double* mixed_max1_max2, int64_t nbatch, ddcb_stream stream);
 /* SplineEvaluator2D::operator() (order1 = order2 = 0, with the periodic wraps / extrapolation rules)
  * and deriv_dim_1 / deriv_dim_2 / deriv_1_and_2 (orders 0 or 1, no boundary handling)
  * (spline_evaluator_2d.hpp:376-598): coords (npoints, nbatch) pairs (x1, x2) -> out (npoints, nbatch);
