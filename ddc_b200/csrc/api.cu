@@ -475,6 +475,116 @@ ddcb_status ddcb_integrate(ddcb_evaluator h, double* out, int64_t out_outer_stri
     });
 }
 
+// Validates the cotangent outputs of the builder adjoint; clears the derivative pointers the
+// closures have no values for.
+static void check_build_adjoint_outputs(ddcb::Builder const& b, ddcb_lines lgv, double*& gdlo, ddcb_lines lglo,
+                                        double*& gdhi, ddcb_lines lghi)
+{
+    if (b.lo == DDCB_HERMITE && b.nbv_lo > 0 && gdlo) {
+        check_lines(lglo, b.nbv_lo, "g_derivs_lo");
+        same_batch(lglo, lgv, "g_derivs_lo/g_vals");
+    } else {
+        gdlo = nullptr;
+    }
+    if (b.hi == DDCB_HERMITE && b.nbv_hi > 0 && gdhi) {
+        check_lines(lghi, b.nbv_hi, "g_derivs_hi");
+        same_batch(lghi, lgv, "g_derivs_hi/g_vals");
+    } else {
+        gdhi = nullptr;
+    }
+}
+
+static void check_device(int device, char const* what)
+{
+    int dev = 0;
+    DDCB_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev != device) throw ddcb::Error(DDCB_ERR_INVALID_ARGUMENT, std::string(what) + " was created for another device");
+}
+
+ddcb_status ddcb_build_adjoint(ddcb_builder h, const double* gc, ddcb_lines lgc, double* gv, ddcb_lines lgv,
+                               double* gdlo, ddcb_lines lglo, double* gdhi, ddcb_lines lghi, ddcb_stream stream)
+{
+    return guarded([&] {
+        require(h != nullptr, "builder is NULL");
+        ddcb::Builder const& b = *h->b;
+        check_lines(lgv, int64_t(b.points.size()), "g_vals");
+        check_lines(lgc, b.basis.size(), "g_coefs");
+        same_batch(lgv, lgc, "g_coefs/g_vals");
+        if (lgv.inner * lgv.outer == 0) return;
+        require(gv && gc, "g_vals/g_coefs pointer is NULL");
+        check_build_adjoint_outputs(b, lgv, gdlo, lglo, gdhi, lghi);
+        check_device(b.device, "the builder");
+        ddcb::launch_build_adjoint(b, gc, ddcb::to_lines(lgc), gv, ddcb::to_lines(lgv), gdlo, ddcb::to_lines(lglo), gdhi,
+                                   ddcb::to_lines(lghi), reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+// Validates the evaluator-side arguments of an adjoint call (coords, g_out, and coefs / g_coords
+// when the coordinate cotangents are wanted).
+static void check_eval_adjoint(ddcb::Evaluator const& e, int order, ddcb_lines lx, const double* coefs, ddcb_lines lc,
+                               ddcb_lines lgy, const double* gx, ddcb_lines lgx)
+{
+    require(order == 0 || order == 1, "the adjoint covers order 0 (values) and 1 (first derivatives)");
+    require(order <= e.basis.desc.degree, "derivative order must be in 0..degree");
+    check_lines(lx, lx.n, "coords");
+    check_lines(lgy, lx.n, "g_out");
+    same_batch(lx, lgy, "coords/g_out");
+    if (gx) {
+        require(coefs != nullptr, "coefs is required for g_coords");
+        check_lines(lc, e.basis.size(), "coefs");
+        check_lines(lgx, lx.n, "g_coords");
+        same_batch(lx, lc, "coords/coefs");
+        same_batch(lx, lgx, "coords/g_coords");
+    }
+    check_device(e.device, "the evaluator");
+}
+
+ddcb_status ddcb_eval_adjoint(ddcb_evaluator he, int32_t order, const double* coords, ddcb_lines lx, const double* coefs,
+                              ddcb_lines lc, const double* gy, ddcb_lines lgy, double* gc, ddcb_lines lgc, double* gx,
+                              ddcb_lines lgx, ddcb_stream stream)
+{
+    return guarded([&] {
+        require(he != nullptr, "evaluator is NULL");
+        ddcb::Evaluator const& e = *he->e;
+        check_lines(lgc, e.basis.size(), "g_coefs");
+        same_batch(lx, lgc, "coords/g_coefs");
+        if (lx.inner * lx.outer == 0) return;
+        check_eval_adjoint(e, order, lx, coefs, lc, lgy, gx, lgx);
+        require(gc != nullptr && (coords && gy || lx.n == 0), "NULL data pointer");
+        ddcb::launch_eval_adjoint(e, order, coords, ddcb::to_lines(lx), coefs, ddcb::to_lines(lc), gy, ddcb::to_lines(lgy),
+                                  gc, ddcb::to_lines(lgc), gx, ddcb::to_lines(lgx), reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+ddcb_status ddcb_build_eval_adjoint(ddcb_builder h, ddcb_evaluator he, int32_t order, const double* coords,
+                                    ddcb_lines lx, const double* coefs, ddcb_lines lc, const double* gy, ddcb_lines lgy,
+                                    double* gv, ddcb_lines lgv, double* gdlo, ddcb_lines lglo, double* gdhi,
+                                    ddcb_lines lghi, double* gx, ddcb_lines lgx, int32_t* fused, ddcb_stream stream)
+{
+    return guarded([&] {
+        if (fused) *fused = 0;
+        require(h != nullptr, "builder is NULL");
+        require(he != nullptr, "evaluator is NULL");
+        ddcb::Builder const& b = *h->b;
+        ddcb::Evaluator const& e = *he->e;
+        require(e.basis.desc.degree == b.basis.desc.degree && e.basis.desc.ncells == b.basis.desc.ncells
+                    && e.basis.desc.uniform == b.basis.desc.uniform && e.basis.desc.periodic == b.basis.desc.periodic,
+                "builder and evaluator use different bases");
+        check_lines(lgv, int64_t(b.points.size()), "g_vals");
+        same_batch(lx, lgv, "coords/g_vals");
+        if (lgv.inner * lgv.outer == 0) return;
+        require(gv != nullptr && (coords && gy || lx.n == 0), "NULL data pointer");
+        check_eval_adjoint(e, order, lx, coefs, lc, lgy, gx, lgx);
+        check_build_adjoint_outputs(b, lgv, gdlo, lglo, gdhi, lghi);
+        check_device(b.device, "the builder");
+        bool const f = ddcb::launch_build_eval_adjoint(
+            b, e, order, coords, ddcb::to_lines(lx), coefs, ddcb::to_lines(lc), gy, ddcb::to_lines(lgy), gv,
+            ddcb::to_lines(lgv), gdlo, ddcb::to_lines(lglo), gdhi, ddcb::to_lines(lghi), gx, ddcb::to_lines(lgx),
+            reinterpret_cast<cudaStream_t>(stream));
+        if (fused) *fused = f ? 1 : 0;
+    });
+}
+
 ddcb_status ddcb_build2d_workspace_bytes(ddcb_builder b1, ddcb_builder b2, int64_t nbatch, uint64_t* bytes)
 {
     return guarded([&] {

@@ -144,23 +144,15 @@ __device__ __forceinline__ void carry_scan(const double* __restrict__ P, double*
     }
 }
 
-// Steps 1-4 of a build: gather the right-hand side rows (spline_builder.hpp:952-1052), forward and
-// backward sweeps, border correction. On return (after a barrier) T[j*TL + l] holds solution
-// column j of line l, for j < n.
-template <int TL, int KL, int KU>
-__device__ __forceinline__ void solve_tile(BuildArgs const& args, double* smem)
+// Step 1 of a build: gather the right-hand side rows of the tile (spline_builder.hpp:952-1052).
+// Tile row r holds system row (r + lrot) mod n; values arrive by async copies, Hermite rows are
+// scaled by dx^k. Ends with a barrier.
+template <int TL>
+__device__ __forceinline__ void gather_tile(BuildArgs const& args, double* T)
 {
-    SolveTables const& t = args.t;
     RhsMap const& R = args.r;
-    constexpr int KC = KL > KU ? KL : KU;
-    int const n = t.n, m = t.m, k = t.k;
-    int const NC = t.nchunk;
+    int const n = args.t.n;
     int const nct = args.nct;
-    double* T = smem;                              // n x TL
-    double* carry = T + (size_t)n * TL;            // NC x KC x TL
-    double* halo = carry + (size_t)NC * KC * TL;   // NC x KL x TL
-    double* btmp = halo + (size_t)NC * KL * TL;    // k x TL
-
     int const tid = threadIdx.x;
     int const l = tid % TL;
     int const c = tid / TL;
@@ -192,6 +184,24 @@ __device__ __forceinline__ void solve_tile(BuildArgs const& args, double* smem)
         cp_async_wait_all();
     }
     __syncthreads();
+}
+
+// Steps 2-4 of a solve on a tile already in shared memory (T[j*TL + l] = right-hand side row j of
+// line l): forward and backward sweeps, border correction. On return (after a barrier) T holds the
+// solution. Every thread of the block must call it.
+template <int TL, int KL, int KU>
+__device__ __forceinline__ void solve_in_tile(SolveTables const& t, int nct, double* smem)
+{
+    constexpr int KC = KL > KU ? KL : KU;
+    int const n = t.n, m = t.m, k = t.k;
+    int const NC = t.nchunk;
+    double* T = smem;                              // n x TL
+    double* carry = T + (size_t)n * TL;            // NC x KC x TL
+    double* halo = carry + (size_t)NC * KC * TL;   // NC x KL x TL
+    double* btmp = halo + (size_t)NC * KL * TL;    // k x TL
+    int const tid = threadIdx.x;
+    int const l = tid % TL;
+    int const c = tid / TL;
 
     int a = 0, e = 0;
     if (c < NC) {
@@ -271,6 +281,15 @@ __device__ __forceinline__ void solve_tile(BuildArgs const& args, double* smem)
         }
         __syncthreads();
     }
+}
+
+// Steps 1-4 of a build. On return (after a barrier) T[j*TL + l] holds solution column j of line l,
+// for j < n.
+template <int TL, int KL, int KU>
+__device__ __forceinline__ void solve_tile(BuildArgs const& args, double* smem)
+{
+    gather_tile<TL>(args, smem);
+    solve_in_tile<TL, KL, KU>(args.t, args.nct, smem);
 }
 
 // Tile row holding output row b: the solution of tile column j belongs to B-spline

@@ -166,6 +166,19 @@ bool launch_build_eval(Builder const& b, Evaluator const& e, int order, double* 
                        double const* vals, Lines const& lv, double const* dlo, Lines const& llo, double const* dhi,
                        Lines const& lhi, double const* coords, Lines const& lx, double* out, Lines const& lo, cudaStream_t s);
 
+// adjoint_kernels.cu
+void launch_build_adjoint(Builder const& b, double const* gc, Lines const& lgc, double* gv, Lines const& lgv,
+                          double* gdlo, Lines const& lglo, double* gdhi, Lines const& lghi, cudaStream_t s);
+void launch_eval_adjoint(Evaluator const& e, int order, double const* coords, Lines const& lx, double const* coefs,
+                         Lines const& lc, double const* gy, Lines const& lgy, double* gc, Lines const& lgc, double* gx,
+                         Lines const& lgx, cudaStream_t s);
+// Returns whether the single fused kernel ran (else the two kernels above did, through a
+// stream-ordered cotangent buffer).
+bool launch_build_eval_adjoint(Builder const& b, Evaluator const& e, int order, double const* coords, Lines const& lx,
+                               double const* coefs, Lines const& lc, double const* gy, Lines const& lgy, double* gv,
+                               Lines const& lgv, double* gdlo, Lines const& lglo, double* gdhi, Lines const& lghi,
+                               double* gx, Lines const& lgx, cudaStream_t s);
+
 // tensor2d.cu
 size_t build2d_workspace_bytes(Builder const& b1, Builder const& b2, int64_t nbatch);
 void launch_build2d(Builder const& b1, Builder const& b2, double* coefs, double const* vals, double const* dmin1,

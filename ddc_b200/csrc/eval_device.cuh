@@ -112,6 +112,34 @@ __device__ __forceinline__ void nonuniform_values_span(const double* kn, const d
     }
 }
 
+// As nonuniform_values_span, also returning the degree P-1 values of the same cell (the level
+// before the last of the triangle), which the spline derivative needs.
+template <int P>
+__device__ __forceinline__ void nonuniform_values_span2(const double* kn, const double* ispan, int nk, double x, double* v,
+                                                        double* vprev)
+{
+    double left[P + 1], right[P + 1];
+    v[0] = 1.0;
+    if (P == 1) vprev[0] = 1.0;
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+        left[j] = x - kn[P - 1 - j];
+        right[j] = kn[P + j] - x;
+        double saved = 0.0;
+#pragma unroll
+        for (int r = 0; r < j + 1; ++r) {
+            double const temp = v[r] * __ldg(ispan + j * nk + r - j);
+            v[r] = saved + right[r] * temp;
+            saved = left[j - r] * temp;
+        }
+        v[j + 1] = saved;
+        if (j == P - 2) {
+#pragma unroll
+            for (int r = 0; r < P; ++r) vprev[r] = v[r];
+        }
+    }
+}
+
 // s(x) without boundary handling (spline_evaluator.hpp:556-605).
 template <int D, bool UNI, class Acc>
 __device__ __forceinline__ double eval_value_no_bc(EvalBasis const& eb, double x, Acc const& C)
@@ -270,6 +298,67 @@ __device__ __forceinline__ int basis_derivs(EvalBasis const& eb, double x, doubl
 #pragma unroll
     for (int i = 0; i <= D; ++i) val[i] = w[i];
     return jmin;
+}
+
+// Reverse mode of one evaluated point. For y = s(x) (ORDER 0, with the boundary handling of
+// eval_value_bc) or y = s'(x) (ORDER 1, no boundary handling), returns the first B-spline index
+// jmin and the weights wts[i] = dy/dc[jmin+i] (the B-spline values, or their derivatives), and sets
+// dydx = dy/dx (s'(x) or s''(x); 0 where y does not depend on x). Returns -1 when y is identically
+// 0 there (null extrapolation). dydx is computed only when want_dx is set.
+template <int D, int ORDER, bool UNI, class Acc>
+__device__ __forceinline__ int point_adjoint(EvalBasis const& eb, int ex_lo, int ex_hi, double x, Acc const& C,
+                                             bool want_dx, double* wts, double& dydx)
+{
+    dydx = 0.0;
+    if constexpr (ORDER == 0) {
+        bool fixed = false; // y does not move with x (constant extrapolation)
+        if (eb.b.periodic) {
+            x = periodic_wrap(eb.b, x);
+        } else if (x < eb.b.rmin) {
+            if (ex_lo == 1) return -1;
+            x = eb.b.rmin;
+            fixed = true;
+        } else if (x > eb.b.rmax) {
+            if (ex_hi == 1) return -1;
+            x = eb.b.rmax;
+            fixed = true;
+        }
+        double vp[D > 1 ? D : 1];
+        int jmin;
+        if (UNI) {
+            double off;
+            jmin = uniform_cell(eb.b, x, off);
+            uniform_values_t<D>(off, wts);
+            uniform_values_t<D - 1>(off, vp);
+        } else {
+            int const ck = nonuniform_locate(eb, x);
+            jmin = ck - D;
+            double kn[2 * D];
+            load_knots<D>(eb, ck, kn);
+            nonuniform_values_span2<D>(kn, eb.inv_span + ck, eb.nk, x, wts, vp);
+        }
+        if (want_dx && !fixed) {
+            // s'(x) = sum_r cc[r+1] B_{jmin+1+r, D-1}(x), cc the first divided differences
+            int const r0 = C.row0(jmin);
+            double cprev = C.get(r0, 0);
+            double y = 0.0;
+#pragma unroll
+            for (int i = 1; i <= D; ++i) {
+                double const ci = C.get(r0, i);
+                double const f = UNI ? eb.b.inv_step : double(D) * __ldg(eb.inv_span + (D - 1) * eb.nk + jmin + i);
+                y = fma((ci - cprev) * f, vp[i - 1], y);
+                cprev = ci;
+            }
+            dydx = y;
+        }
+        return jmin;
+    } else {
+        int const jmin = basis_derivs<D, ORDER, UNI>(eb, x, wts);
+        if constexpr (ORDER + 1 <= D) {
+            if (want_dx) dydx = eval_deriv_no_bc<D, ORDER + 1, UNI>(eb, x, C);
+        }
+        return jmin;
+    }
 }
 
 #endif

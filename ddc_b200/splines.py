@@ -230,6 +230,42 @@ class SplineBuilder:
                   lines_of(out, dim), C.byref(fused), _stream_handle(stream))
         return bool(fused.value)
 
+    def adjoint(self, g_spline, g_vals, g_derivs_xmin=None, g_derivs_xmax=None, *, dim: int = 0, stream=None):
+        """Reverse mode of operator(): given the cotangents g_spline of the coefficients, writes the
+        cotangents of vals (and of the Hermite derivatives, when tensors are given) -- the transposed
+        solve of the interpolation matrix with the periodic duplicates folded back."""
+        gc = _dev_f64(g_spline, "g_spline")
+        gv = _dev_f64(g_vals, "g_vals")
+        glo = _dev_f64(g_derivs_xmin, "g_derivs_xmin")
+        ghi = _dev_f64(g_derivs_xmax, "g_derivs_xmax")
+        llo = lines_of(glo, dim) if glo is not None else Lines(0, 1, 0, 0, 0)
+        lhi = lines_of(ghi, dim) if ghi is not None else Lines(0, 1, 0, 0, 0)
+        _lib.call("ddcb_build_adjoint", self._h, _ptr(gc), lines_of(gc, dim), _ptr(gv), lines_of(gv, dim), _ptr(glo),
+                  llo, _ptr(ghi), lhi, _stream_handle(stream))
+        return gv
+
+    def build_and_evaluate_adjoint(self, evaluator: "SplineEvaluator", coords_eval, spline_coef, g_spline_eval, g_vals,
+                                   g_coords=None, g_derivs_xmin=None, g_derivs_xmax=None, *, order: int = 0,
+                                   dim: int = 0, stream=None) -> bool:
+        """Reverse mode of build_and_evaluate: from the cotangents of the evaluated values, the
+        cotangents of vals (and Hermite derivatives) and, when g_coords is given, of the coordinates
+        (spline_coef is then read). Returns True when one fused kernel ran."""
+        x = _dev_f64(coords_eval, "coords_eval")
+        c = _dev_f64(spline_coef, "spline_coef")
+        gy = _dev_f64(g_spline_eval, "g_spline_eval")
+        gv = _dev_f64(g_vals, "g_vals")
+        gx = _dev_f64(g_coords, "g_coords")
+        glo = _dev_f64(g_derivs_xmin, "g_derivs_xmin")
+        ghi = _dev_f64(g_derivs_xmax, "g_derivs_xmax")
+        empty = Lines(0, 1, 0, 0, 0)
+        fused = C.c_int32(0)
+        _lib.call("ddcb_build_eval_adjoint", self._h, evaluator._h, int(order), _ptr(x), lines_of(x, dim), _ptr(c),
+                  lines_of(c, dim) if c is not None else empty, _ptr(gy), lines_of(gy, dim), _ptr(gv), lines_of(gv, dim),
+                  _ptr(glo), lines_of(glo, dim) if glo is not None else empty, _ptr(ghi),
+                  lines_of(ghi, dim) if ghi is not None else empty, _ptr(gx),
+                  lines_of(gx, dim) if gx is not None else empty, C.byref(fused), _stream_handle(stream))
+        return bool(fused.value)
+
     def solve(self, rhs, transpose: bool = False, stream=None):
         """In-place SplinesLinearProblem::solve on a (nbasis, nrhs) CUDA float64 matrix."""
         rhs = _dev_f64(rhs, "rhs")
@@ -285,6 +321,22 @@ class SplineEvaluator:
         _lib.call("ddcb_eval_deriv", self._h, int(order), _ptr(out), lines_of(out, dim), _ptr(x), lines_of(x, dim),
                   _ptr(c), lines_of(c, dim), _stream_handle(stream))
         return out
+
+    def adjoint(self, coords_eval, g_spline_eval, g_spline_coef, spline_coef=None, g_coords=None, *, order: int = 0,
+                dim: int = 0, stream=None):
+        """Reverse mode of operator() (order 0) / deriv(1, ...) (order 1): writes g_spline_coef, the
+        cotangents of the coefficients (a scatter-add of basis-weighted cotangents), and, when
+        g_coords is given, the cotangents of the coordinates (needs spline_coef)."""
+        x = _dev_f64(coords_eval, "coords_eval")
+        gy = _dev_f64(g_spline_eval, "g_spline_eval")
+        gc = _dev_f64(g_spline_coef, "g_spline_coef")
+        c = _dev_f64(spline_coef, "spline_coef")
+        gx = _dev_f64(g_coords, "g_coords")
+        empty = Lines(0, 1, 0, 0, 0)
+        _lib.call("ddcb_eval_adjoint", self._h, int(order), _ptr(x), lines_of(x, dim), _ptr(c),
+                  lines_of(c, dim) if c is not None else empty, _ptr(gy), lines_of(gy, dim), _ptr(gc),
+                  lines_of(gc, dim), _ptr(gx), lines_of(gx, dim) if gx is not None else empty, _stream_handle(stream))
+        return gc
 
     def integrate(self, integrals, spline_coef, *, dim: int = 0, stream=None):
         """SplineEvaluator::integrate(integrals, spline_coef): integrals has the batch shape of spline_coef."""

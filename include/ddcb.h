@@ -167,6 +167,35 @@ ddcb_status ddcb_build_eval(ddcb_builder b, ddcb_evaluator e, int32_t order, dou
                             const double* coords, ddcb_lines coords_layout, double* out, ddcb_lines out_layout,
                             int32_t* fused, ddcb_stream stream);
 
+/* ---- reverse mode (no reference counterpart: the reference has no derivatives with respect to
+ *      its inputs). The builder is linear, coefs = P A^-1 R (vals, dx^k derivs); the evaluator is
+ *      y = sum_i c[jmin+i] B_i(x). Every cotangent output is overwritten, not accumulated. ---- */
+/* Adjoint of ddcb_build: g_vals = R^T A^-T P^T g_coefs, with the cotangents of the periodic
+ * duplicate coefficients folded back (spline_builder.hpp:1073-1100) and the transposed solve of
+ * SplinesLinearProblem::solve(b, true) (splines_linear_problem.hpp:80-92). g_derivs_lo/hi (nbv_lo,
+ * nbv_hi rows) receive the cotangents of the Hermite derivatives; either may be NULL. */
+ddcb_status ddcb_build_adjoint(ddcb_builder b, const double* g_coefs, ddcb_lines g_coefs_layout, double* g_vals,
+                               ddcb_lines g_vals_layout, double* g_derivs_lo, ddcb_lines g_derivs_lo_layout,
+                               double* g_derivs_hi, ddcb_lines g_derivs_hi_layout, ddcb_stream stream);
+/* Adjoint of ddcb_eval (order 0) / ddcb_eval_deriv (order 1): g_coefs[jmin+i] = sum over the
+ * line's points of g_out * d out / d c[jmin+i], and g_coords = g_out * d out / dx (the spline
+ * derivative of order + 1; 0 outside the domain where the extrapolation rule is constant or null).
+ * coefs is read only for g_coords, which may be NULL (then coefs may be NULL too). */
+ddcb_status ddcb_eval_adjoint(ddcb_evaluator e, int32_t order, const double* coords, ddcb_lines coords_layout,
+                              const double* coefs, ddcb_lines coefs_layout, const double* g_out, ddcb_lines g_out_layout,
+                              double* g_coefs, ddcb_lines g_coefs_layout, double* g_coords, ddcb_lines g_coords_layout,
+                              ddcb_stream stream);
+/* Backward of ddcb_build_eval: the evaluator adjoint scattered straight into the transposed solve
+ * of the builder adjoint, so g_coefs never reaches memory. g_vals, g_derivs_lo/hi as in
+ * ddcb_build_adjoint, g_coords as in ddcb_eval_adjoint; *fused (may be NULL) tells whether one
+ * kernel did both. */
+ddcb_status ddcb_build_eval_adjoint(ddcb_builder b, ddcb_evaluator e, int32_t order, const double* coords,
+                                    ddcb_lines coords_layout, const double* coefs, ddcb_lines coefs_layout,
+                                    const double* g_out, ddcb_lines g_out_layout, double* g_vals,
+                                    ddcb_lines g_vals_layout, double* g_derivs_lo, ddcb_lines g_derivs_lo_layout,
+                                    double* g_derivs_hi, ddcb_lines g_derivs_hi_layout, double* g_coords,
+                                    ddcb_lines g_coords_layout, int32_t* fused, ddcb_stream stream);
+
 /* ---- 2D tensor product: SplineBuilder2D / SplineEvaluator2D on two 1D plans, for the layout
  *      (x1, x2, batch) with the batch contiguous (the reference's layout_right of
  *      DiscreteDomain<X1, X2, batch...>). ----------------------------------------------------- */
