@@ -19,6 +19,7 @@
 // directly in the tile of the transposed solve, so neither g_coefs nor the coefficients' tile
 // round-trips through HBM.
 #include <algorithm>
+#include <type_traits>
 
 #include "build_device.cuh"
 #include "eval_device.cuh"
@@ -28,12 +29,6 @@ namespace ddcb {
 namespace {
 
 constexpr int kAdjThreads = 512;
-
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
-{
-    unsigned const s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
-}
 
 // Cotangent tile rows of B-spline jmin + i: the coefficient row itself (RowsDirect) or the column
 // of the solve it came from (RowsRotated, the inverse of coef_row; duplicates fold automatically).
@@ -151,6 +146,7 @@ struct EvalAdjointArgs
     Lines lx;
     const double* coefs;    // needed for g_coords only
     Lines lc;
+    int coef_pairs;         // coefs: adjacent line pairs 16-byte aligned and contiguous
     const double* gy;       // cotangents of the evaluated values
     Lines lgy;
     double* gc;             // out: cotangents of the coefficients (standalone kernel)
@@ -159,40 +155,77 @@ struct EvalAdjointArgs
     Lines lgx;
 };
 
-// Shared-memory prologue of the evaluator part: the coefficient tile (when g_x is wanted) and the
-// knot pairs (non-uniform), as async copies; the caller waits and synchronises.
-template <int TLE, bool UNI>
-__device__ __forceinline__ void load_eval_tiles(EvalAdjointArgs const& a, double* C, double2* K, int nct)
+// The knot pairs (non-uniform bases) into shared memory, as async copies.
+template <bool UNI>
+__device__ __forceinline__ void load_knot_pairs(EvalAdjointArgs const& a, double2* K)
 {
-    int const tid = threadIdx.x;
-    int const l = tid % TLE;
-    int const c = tid / TLE;
-    int64_t const line = (int64_t)blockIdx.x * TLE + l;
-    if (a.gx && line < a.nlines) {
-        int64_t const oc = line_offset(a.lc, line);
-        for (int r = c; r < a.size; r += nct) cp_async8(C + r * TLE + l, a.coefs + r * a.lc.stride + oc);
-    }
     if (!UNI)
-        for (int i = tid; i < a.eb.nk - 1; i += blockDim.x) cp_async16(K + i, a.eb.kpairs + i);
+        for (int i = threadIdx.x; i < a.eb.nk - 1; i += blockDim.x) cp_async16(K + i, a.eb.kpairs + i);
 }
 
-// Points of line l handled by this thread: scatter g_y * B into G (rows from Rows), write g_x.
-template <int D, int TLE, int ORDER, bool UNI, class Rows>
-__device__ __forceinline__ void scatter_points(EvalAdjointArgs const& a, EvalBasis const& eb, const double* C, double* G,
-                                               Rows const& rows, int nct)
+// The coefficient tile of the block's TLE lines into C (row r of line l at C[r*TLE + l]), as async
+// copies: two lines per 16-byte copy where the layout allows.
+template <int TLE>
+__device__ __forceinline__ void load_coef_tile(EvalAdjointArgs const& a, double* C)
+{
+    int const tid = threadIdx.x;
+    if (TLE % 2 == 0 && a.coef_pairs) {
+        int const p = tid % (TLE / 2);
+        int const c2 = tid / (TLE / 2);
+        int const step = blockDim.x / (TLE / 2);
+        int64_t const l0 = (int64_t)blockIdx.x * TLE + 2 * p;
+        if (l0 + 1 < a.nlines) {
+            int64_t const oc = line_offset(a.lc, l0);
+            for (int r = c2; r < a.size; r += step) cp_async16(C + r * TLE + 2 * p, a.coefs + r * a.lc.stride + oc);
+        } else if (l0 < a.nlines) {
+            int64_t const oc = line_offset(a.lc, l0);
+            for (int r = c2; r < a.size; r += step) cp_async8(C + r * TLE + 2 * p, a.coefs + r * a.lc.stride + oc);
+        }
+        return;
+    }
+    int const l = tid % TLE;
+    int const c = tid / TLE;
+    int const step = blockDim.x / TLE;
+    int64_t const line = (int64_t)blockIdx.x * TLE + l;
+    if (line >= a.nlines) return;
+    int64_t const oc = line_offset(a.lc, line);
+    for (int r = c; r < a.size; r += step) cp_async8(C + r * TLE + l, a.coefs + r * a.lc.stride + oc);
+}
+
+// dy/dx of one evaluated point: s'(x) for a value (ORDER 0) with the boundary handling of
+// eval_value_bc (0 outside the domain, where null and constant extrapolation do not move with x),
+// or the next derivative for a derivative (ORDER 1, no boundary handling).
+template <int D, int ORDER, bool UNI, class Acc>
+__device__ __forceinline__ double point_dydx(EvalBasis const& eb, double x, Acc const& C)
+{
+    if constexpr (ORDER == 0) {
+        if (eb.b.periodic) x = periodic_wrap(eb.b, x);
+        else if (x < eb.b.rmin || x > eb.b.rmax) return 0.0;
+        return eval_deriv_no_bc<D, 1, UNI>(eb, x, C);
+    } else if constexpr (ORDER + 1 <= D) {
+        return eval_deriv_no_bc<D, ORDER + 1, UNI>(eb, x, C);
+    } else {
+        return 0.0;
+    }
+}
+
+// Phase 1 of an evaluator adjoint: g_x = g_y * dy/dx for the points of the thread's line, with the
+// line's coefficients in the shared tile C.
+template <int D, int TLE, int ORDER, bool UNI>
+__device__ __forceinline__ void coord_cotangents(EvalAdjointArgs const& a, EvalBasis const& eb, const double* C)
 {
     int const tid = threadIdx.x;
     int const l = tid % TLE;
     int const c = tid / TLE;
+    int const nct = blockDim.x / TLE;
     int64_t const line = (int64_t)blockIdx.x * TLE + l;
     if (line >= a.nlines) return;
     int64_t const ox = line_offset(a.lx, line);
     int64_t const og = line_offset(a.lgy, line);
-    int64_t const m = a.lx.n;
-    bool const want_dx = a.gx != nullptr;
-    int64_t const oxo = want_dx ? line_offset(a.lgx, line) : 0;
+    int64_t const oxo = line_offset(a.lgx, line);
     CoefDirect const acc {C + l, TLE};
     constexpr int U = 8; // points in flight per thread
+    int64_t const m = a.lx.n;
     int const npt = m > c ? int((m - c + nct - 1) / nct) : 0;
     for (int q0 = 0; q0 < npt; q0 += U) {
         double xs[U], gs[U];
@@ -203,63 +236,112 @@ __device__ __forceinline__ void scatter_points(EvalAdjointArgs const& a, EvalBas
             gs[u] = (q0 + u < npt) ? a.gy[p * a.lgy.stride + og] : 0.0;
         }
 #pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (q0 + u < npt)
+                __stcs(a.gx + (c + int64_t(q0 + u) * nct) * a.lgx.stride + oxo, gs[u] * point_dydx<D, ORDER, UNI>(eb, xs[u], acc));
+    }
+}
+
+// Phase 2: scatter g_y * dy/dc into the cotangent tile G (rows from Rows). The coordinates and
+// cotangents are read a second time; the block read them just before, so they come from L2.
+template <int D, int TLE, int ORDER, bool UNI, class Rows>
+__device__ __forceinline__ void scatter_points(EvalAdjointArgs const& a, EvalBasis const& eb, double* G, Rows const& rows)
+{
+    int const tid = threadIdx.x;
+    int const l = tid % TLE;
+    int const c = tid / TLE;
+    int const nct = blockDim.x / TLE;
+    int64_t const line = (int64_t)blockIdx.x * TLE + l;
+    if (line >= a.nlines) return;
+    int64_t const ox = line_offset(a.lx, line);
+    int64_t const og = line_offset(a.lgy, line);
+    CoefDirect const none {nullptr, 0};
+    constexpr int U = 8;
+    int64_t const m = a.lx.n;
+    int const npt = m > c ? int((m - c + nct - 1) / nct) : 0;
+    for (int q0 = 0; q0 < npt; q0 += U) {
+        double xs[U], gs[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            int64_t const p = c + int64_t(q0 + u) * nct;
+            xs[u] = (q0 + u < npt) ? __ldcs(a.coords + p * a.lx.stride + ox) : 0.0;
+            gs[u] = (q0 + u < npt) ? __ldcs(a.gy + p * a.lgy.stride + og) : 0.0;
+        }
+#pragma unroll
         for (int u = 0; u < U; ++u) {
             if (q0 + u >= npt) continue;
-            double w[D + 1], dydx;
-            int const jmin = point_adjoint<D, ORDER, UNI>(eb, a.ex_lo, a.ex_hi, xs[u], acc, want_dx, w, dydx);
+            double w[D + 1], unused;
+            int const jmin = point_adjoint<D, ORDER, UNI>(eb, a.ex_lo, a.ex_hi, xs[u], none, false, w, unused);
             if (jmin >= 0) {
                 int const r0 = rows.row0(jmin);
 #pragma unroll
                 for (int i = 0; i < D + 1; ++i) atomicAdd(G + rows.row(r0, i) * TLE + l, gs[u] * w[i]);
             }
-            if (want_dx) a.gx[(c + int64_t(q0 + u) * nct) * a.lgx.stride + oxo] = gs[u] * dydx;
         }
     }
 }
 
+// Evaluator adjoint. One shared tile serves twice: first as the coefficient tile for g_x, then as
+// the cotangent tile the scatter accumulates into.
 template <int D, int TLE, int ORDER, bool UNI>
 __global__ void __launch_bounds__(kAdjThreads) eval_adjoint_kernel(const __grid_constant__ EvalAdjointArgs a)
 {
     extern __shared__ __align__(16) double smem[];
-    double* G = smem;                                   // size x TLE cotangent tile
-    double* C = G + (size_t)a.size * TLE;               // size x TLE coefficient tile
-    // knot pairs at an even double offset (16-byte aligned)
-    double2* K = reinterpret_cast<double2*>(smem + (((size_t)a.size * TLE * (a.gx ? 2 : 1) + 1) & ~size_t(1)));
-    int const nct = blockDim.x / TLE;
-    load_eval_tiles<TLE, UNI>(a, C, K, nct);
-    for (int i = threadIdx.x; i < a.size * TLE; i += blockDim.x) G[i] = 0.0;
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    double* G = smem;                                                  // size x TLE
+    double2* K = reinterpret_cast<double2*>(smem + (((size_t)a.size * TLE + 1) & ~size_t(1)));
+    load_knot_pairs<UNI>(a, K);
+    if (a.gx) load_coef_tile<TLE>(a, G);
+    cp_async_wait_all();
     __syncthreads();
     EvalBasis eb = a.eb;
     if (!UNI) eb.kpairs = K;
-    scatter_points<D, TLE, ORDER, UNI>(a, eb, C, G, RowsDirect {}, nct);
+    if (a.gx) {
+        coord_cotangents<D, TLE, ORDER, UNI>(a, eb, G);
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < a.size * TLE; i += blockDim.x) G[i] = 0.0;
+    __syncthreads();
+    scatter_points<D, TLE, ORDER, UNI>(a, eb, G, RowsDirect {});
     __syncthreads();
     int const l = threadIdx.x % TLE;
     int const c = threadIdx.x / TLE;
+    int const nct = blockDim.x / TLE;
     int64_t const line = (int64_t)blockIdx.x * TLE + l;
     if (line >= a.nlines) return;
     int64_t const og = line_offset(a.lgc, line);
-    for (int r = c; r < a.size; r += nct) a.gc[r * a.lgc.stride + og] = G[r * TLE + l];
+    for (int r = c; r < a.size; r += nct) __stcs(a.gc + r * a.lgc.stride + og, G[r * TLE + l]);
 }
 
-// Backward of build + evaluate: scatter into the transposed solve's tile, solve with A^T, store
-// the sample cotangents.
+// Doubles of the fused kernel's shared tile: the solve tile, or the coefficient tile if larger.
+__host__ __device__ inline size_t fused_tile_doubles(SolveTables const& t, int size, int TL, int KL, int KU)
+{
+    size_t const td = tile_doubles(t, TL, KL, KU);
+    size_t const tc = (size_t)size * TL;
+    return ((td > tc ? td : tc) + 1) & ~size_t(1);
+}
+
+// Backward of build + evaluate: g_x from the coefficient tile, then the scatter into the
+// transposed solve's tile (the same shared memory), the solve with A^T and the sample cotangents.
 template <int TL, int KL, int KU, int D, int ORDER, bool UNI>
 __global__ void __launch_bounds__(1024) build_eval_adjoint_kernel(const __grid_constant__ AdjointArgs a,
                                                                   const __grid_constant__ EvalAdjointArgs ea)
 {
     extern __shared__ __align__(16) double smem[];
-    size_t const td = (tile_doubles(a.t, TL, KL, KU) + 1) & ~size_t(1);
     double* T = smem;
-    double* C = smem + td;
-    double2* K = reinterpret_cast<double2*>(C + (ea.gx ? (size_t)ea.size * TL : 0));
-    load_eval_tiles<TL, UNI>(ea, C, K, a.nct);
-    for (int i = threadIdx.x; i < a.t.n * TL; i += blockDim.x) T[i] = 0.0;
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    double2* K = reinterpret_cast<double2*>(smem + fused_tile_doubles(a.t, ea.size, TL, KL, KU));
+    load_knot_pairs<UNI>(ea, K);
+    if (ea.gx) load_coef_tile<TL>(ea, T);
+    cp_async_wait_all();
     __syncthreads();
     EvalBasis eb = ea.eb;
     if (!UNI) eb.kpairs = K;
-    scatter_points<D, TL, ORDER, UNI>(ea, eb, C, T, RowsRotated {a.t.n, a.r.srot}, a.nct);
+    if (ea.gx) {
+        coord_cotangents<D, TL, ORDER, UNI>(ea, eb, T);
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < a.t.n * TL; i += blockDim.x) T[i] = 0.0;
+    __syncthreads();
+    scatter_points<D, TL, ORDER, UNI>(ea, eb, T, RowsRotated {a.t.n, a.r.srot});
     __syncthreads();
     solve_in_tile<TL, KL, KU>(a.t, a.nct, smem);
     store_adjoint<TL>(a, smem);
@@ -304,10 +386,10 @@ template <int KL, int KU>
 void launch_build_adjoint_k(AdjointArgs const& a, int TL, cudaStream_t s)
 {
     switch (TL) {
-    case 1: launch_build_adjoint_tl<1, KL, KU>(a, s); break;
+    case 2: launch_build_adjoint_tl<2, KL, KU>(a, s); break;
     case 4: launch_build_adjoint_tl<4, KL, KU>(a, s); break;
     case 8: launch_build_adjoint_tl<8, KL, KU>(a, s); break;
-    default: throw Error(DDCB_ERR_UNSUPPORTED, "tile_lines must be 1, 4 or 8");
+    default: throw Error(DDCB_ERR_UNSUPPORTED, "tile_lines must be 2, 4 or 8");
     }
 }
 
@@ -361,6 +443,7 @@ EvalAdjointArgs make_eval_adjoint_args(Evaluator const& e, double const* coords,
     a.lx = lx;
     a.coefs = coefs;
     a.lc = lc;
+    a.coef_pairs = coefs != nullptr && line_pairs_aligned(coefs, lc);
     a.gy = gy;
     a.lgy = lgy;
     a.gc = gc;
@@ -372,7 +455,7 @@ EvalAdjointArgs make_eval_adjoint_args(Evaluator const& e, double const* coords,
 
 size_t eval_adjoint_smem(EvalAdjointArgs const& a, int TLE, bool uni)
 {
-    return sizeof(double) * (((size_t)a.size * TLE * (a.gx ? 2 : 1) + 1) & ~size_t(1)) + (uni ? 0 : sizeof(double2) * (size_t)a.eb.nk);
+    return sizeof(double) * (((size_t)a.size * TLE + 1) & ~size_t(1)) + (uni ? 0 : sizeof(double2) * (size_t)a.eb.nk);
 }
 
 template <int D, int TLE, bool UNI>
@@ -410,8 +493,7 @@ template <int KL, int KU, int D, int ORDER, bool UNI>
 bool launch_fused5(AdjointArgs const& a, EvalAdjointArgs const& ea, cudaStream_t s)
 {
     constexpr int TL = 8;
-    size_t const td = (tile_doubles(a.t, TL, KL, KU) + 1) & ~size_t(1);
-    size_t const sm = sizeof(double) * (td + (ea.gx ? (size_t)ea.size * TL : 0)) + (UNI ? 0 : sizeof(double2) * (size_t)ea.eb.nk);
+    size_t const sm = sizeof(double) * fused_tile_doubles(a.t, ea.size, TL, KL, KU) + (UNI ? 0 : sizeof(double2) * (size_t)ea.eb.nk);
     if (sm > optin_smem()) return false;
     auto kern = build_eval_adjoint_kernel<TL, KL, KU, D, ORDER, UNI>;
     set_smem(kern, sm);
@@ -459,8 +541,9 @@ void launch_eval_adjoint(Evaluator const& e, int order, double const* coords, Li
 {
     EvalAdjointArgs a = make_eval_adjoint_args(e, coords, lx, coefs, lc, gy, lgy, gc, lgc, gx, lgx);
     if (a.nlines == 0) return;
-    // four lines per block keep two shared tiles of a 1000-row line under a third of an SM
-    if (eval_adjoint_smem(a, 4, a.eb.b.uniform != 0) <= optin_smem()) launch_eval_adjoint_tle<4>(a, order, s);
+    // eight lines per block: the shared tile of a 1000-row line takes under a third of an SM
+    if (eval_adjoint_smem(a, 8, a.eb.b.uniform != 0) <= optin_smem()) launch_eval_adjoint_tle<8>(a, order, s);
+    else if (eval_adjoint_smem(a, 4, a.eb.b.uniform != 0) <= optin_smem()) launch_eval_adjoint_tle<4>(a, order, s);
     else if (eval_adjoint_smem(a, 1, a.eb.b.uniform != 0) <= optin_smem()) launch_eval_adjoint_tle<1>(a, order, s);
     else throw Error(DDCB_ERR_UNSUPPORTED, "coefficient tile of the evaluator adjoint exceeds shared memory");
 }

@@ -35,7 +35,10 @@ struct BuildArgs
     double* out;
     Lines lo;
     int nct;            // chunk threads per line (block = TL * nct)
+    int pair16;         // vals: adjacent line pairs are 16-byte aligned and contiguous
+    int pair16_out;     // out: the same for the coefficient output
 };
+
 
 __device__ __forceinline__ int64_t line_offset(Lines const& L, int64_t b)
 {
@@ -48,6 +51,12 @@ __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src)
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
 }
 
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
+{
+    unsigned const s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // Shared-memory doubles of one tile: the rows, the carries, the halo rows and the border scratch.
@@ -57,88 +66,111 @@ __host__ __device__ inline size_t tile_doubles(SolveTables const& t, int TL, int
     return (size_t)t.n * TL + (size_t)t.nchunk * KC * TL + (size_t)t.nchunk * KL * TL + (size_t)t.k * TL;
 }
 
-template <int KL, bool PIV>
-__device__ __forceinline__ void fwd_sweep(SolveTables const& t, double* T, int TL, int l, int a, int e, double* w,
-                                          bool write, const double* halo, int hstride)
+// Row of the factor tables holding row j: runs of identical rows (the steady state of a
+// constant-coefficient band) are stored once (plan.cpp, upload_tables).
+__device__ __forceinline__ int crow(SolveTables const& t, int j)
 {
-    int const m = t.m;
+    return j < t.cj0 ? j : (j < t.cj1 ? t.cj0 : j - t.cshift);
+}
+
+__device__ __forceinline__ double2 fma2(double a, double2 y, double2 w)
+{
+    return make_double2(fma(a, y.x, w.x), fma(a, y.y, w.y));
+}
+
+// Forward sweep with L (and the row interchanges when PIV) over rows [a, e) of a line pair; T2
+// points at the pair's column (row j at T2[j*P]). w[0..KL-1] hold rows a..a+KL-1 on entry. Phase A
+// (WRITE false) reads rows beyond e from the tile, which nothing has written yet. Phase C (WRITE
+// true) writes rows a..e-1; without interchanges rows beyond e only feed the next chunk's rows,
+// so they are not read; with interchanges they come from the halo copy.
+template <int KL, bool PIV, bool WRITE>
+__device__ __forceinline__ void fwd_sweep(SolveTables const& t, double2* T2, int P, int a, int e, double2* w,
+                                          const double2* halo, int hstride)
+{
+    int const lim = (WRITE && !PIV) ? e : t.m; // fill rows below lim are read
+#pragma unroll 4
     for (int j = a; j < e; ++j) {
         int const rr = j + KL;
-        double fill;
-        if (rr < e) fill = T[rr * TL + l];
-        else if (rr < m) fill = halo ? halo[(rr - e) * hstride] : T[rr * TL + l];
-        else fill = 0.0;
+        double2 fill = make_double2(0.0, 0.0);
+        if (rr < e) fill = T2[rr * P];
+        else if (rr < lim) fill = (WRITE && PIV) ? halo[(rr - e) * hstride] : T2[rr * P];
         w[KL] = fill;
+        int const cj = crow(t, j);
         if (PIV) {
-            int const p = __ldg(t.piv + j);
+            int const pv = __ldg(t.piv + cj);
 #pragma unroll
             for (int q = 1; q <= KL; ++q)
-                if (p == q) {
-                    double const s = w[0];
+                if (pv == q) {
+                    double2 const s = w[0];
                     w[0] = w[q];
                     w[q] = s;
                 }
         }
-        double const y = w[0];
-        if (write) T[j * TL + l] = y;
-        double const* L = t.Lf + (size_t)j * KL;
+        double2 const y = w[0];
+        if (WRITE) T2[j * P] = y;
+        double const* L = t.Lf + (size_t)cj * KL;
 #pragma unroll
-        for (int q = 1; q <= KL; ++q) w[q] = fma(-__ldg(L + q - 1), y, w[q]);
+        for (int q = 1; q <= KL; ++q) w[q] = fma2(-__ldg(L + q - 1), y, w[q]);
 #pragma unroll
         for (int q = 0; q < KL; ++q) w[q] = w[q + 1];
     }
 }
 
-template <int KU>
-__device__ __forceinline__ void bwd_sweep(SolveTables const& t, double* T, int TL, int l, int a, int e, double* z, bool write)
+// Backward sweep with U over rows e-1 .. a of a line pair; z[0..KU-1] hold the solution rows
+// e .. e+KU-1 (the carry from the chunk below) on entry.
+template <int KU, bool WRITE>
+__device__ __forceinline__ void bwd_sweep(SolveTables const& t, double2* T2, int P, int a, int e, double2* z)
 {
+#pragma unroll 4
     for (int j = e - 1; j >= a; --j) {
-        double const* U = t.Uf + (size_t)j * (KU + 1);
-        double s = T[j * TL + l];
+        double const* U = t.Uf + (size_t)crow(t, j) * (KU + 1);
+        double2 s = T2[j * P];
 #pragma unroll
-        for (int q = 1; q <= KU; ++q) s = fma(-__ldg(U + q), z[q - 1], s);
-        double const x = s * __ldg(U);
-        if (write) T[j * TL + l] = x;
+        for (int q = 1; q <= KU; ++q) s = fma2(-__ldg(U + q), z[q - 1], s);
+        double const d = __ldg(U);
+        double2 const x = make_double2(s.x * d, s.y * d);
+        if (WRITE) T2[j * P] = x;
 #pragma unroll
         for (int q = KU - 1; q >= 1; --q) z[q] = z[q - 1];
         z[0] = x;
     }
 }
 
-// Log-depth (Kogge-Stone) scan of the chunk carries. On entry carry[c] holds chunk c's outgoing
-// carry for a zero incoming carry; on exit it holds the true outgoing carry. Forward: chunk c's
-// carry flows into c+1, out(c) = Phi_c out(c-1) + hat(c); step k adds P(k,c) y(c-2^k). Backward:
-// the carry flows from c+1 into c with Q(k,c) y(c+2^k). Every thread of the block takes part in the
-// barriers; threads of chunk c < NC do the arithmetic.
-template <int K, int KC, int TL, bool FWD>
-__device__ __forceinline__ void carry_scan(const double* __restrict__ P, double* carry, int nscan, int NC, int c, int l)
+// Log-depth (Kogge-Stone) scan of the chunk carries of a line pair (carry of chunk c, entry q at
+// C2[(c*KC + q)*P]). On entry carry[c] holds chunk c's outgoing carry for a zero incoming carry;
+// on exit it holds the true outgoing carry. Forward: chunk c's carry flows into c+1,
+// out(c) = Phi_c out(c-1) + hat(c); step k adds P(k,c) y(c-2^k). Backward: the carry flows from
+// c+1 into c with Q(k,c) y(c+2^k). Every thread of the block takes part in the barriers; threads
+// of chunk c < NC do the arithmetic.
+template <int K, int KC, bool FWD>
+__device__ __forceinline__ void carry_scan(const double* __restrict__ Pm, double2* C2, int P, int nscan, int NC, int c)
 {
-    double y[K];
+    double2 y[K];
     bool const act = c < NC;
     if (act) {
 #pragma unroll
-        for (int q = 0; q < K; ++q) y[q] = carry[(c * KC + q) * TL + l];
+        for (int q = 0; q < K; ++q) y[q] = C2[(c * KC + q) * P];
     }
     for (int k = 0; k < nscan; ++k) {
         int const nb = FWD ? c - (1 << k) : c + (1 << k);
         bool const has = act && (FWD ? nb >= 0 : nb < NC);
-        double v[K];
+        double2 v[K];
         if (has) {
 #pragma unroll
-            for (int q = 0; q < K; ++q) v[q] = carry[(nb * KC + q) * TL + l];
+            for (int q = 0; q < K; ++q) v[q] = C2[(nb * KC + q) * P];
         }
         __syncthreads();
         if (has) {
-            double const* M = P + ((size_t)k * NC + c) * K * K;
+            double const* M = Pm + ((size_t)k * NC + c) * K * K;
 #pragma unroll
             for (int r = 0; r < K; ++r) {
-                double s = y[r];
+                double2 s = y[r];
 #pragma unroll
-                for (int q = 0; q < K; ++q) s = fma(__ldg(M + r * K + q), v[q], s);
+                for (int q = 0; q < K; ++q) s = fma2(__ldg(M + r * K + q), v[q], s);
                 y[r] = s;
             }
 #pragma unroll
-            for (int q = 0; q < K; ++q) carry[(c * KC + q) * TL + l] = y[q];
+            for (int q = 0; q < K; ++q) C2[(c * KC + q) * P] = y[q];
         }
         __syncthreads();
     }
@@ -154,54 +186,80 @@ __device__ __forceinline__ void gather_tile(BuildArgs const& args, double* T)
     int const n = args.t.n;
     int const nct = args.nct;
     int const tid = threadIdx.x;
-    int const l = tid % TL;
-    int const c = tid / TL;
-    int64_t const line = (int64_t)blockIdx.x * TL + l;
-    bool const live = line < args.nlines;
+    int const v0 = (args.raw || R.periodic) ? 0 : R.nbe_lo;
+    int const v1 = (args.raw || R.periodic) ? n : R.nbe_lo + R.npoints;
 
     // ---- 1. gather the right-hand side: tile row r holds system row (r + lrot) mod n; values
     //         arrive by async copies, Hermite rows are scaled by dx^k ----
-    {
+    // Rows that are not samples: dx-scaled Hermite derivatives, or 0.
+    auto other_row = [&](int sr, int64_t line) -> double {
+        if (sr < R.nbe_lo) return sr < R.nbv_lo ? args.dlo[sr * args.llo.stride + line_offset(args.llo, line)] * R.dxpow_lo[sr] : 0.0;
+        int const i = sr - (n - R.nbe_hi);
+        return i < R.nbv_hi ? args.dhi[i * args.lhi.stride + line_offset(args.lhi, line)] * R.dxpow_hi[i] : 0.0;
+    };
+    if (TL % 2 == 0 && args.pair16) {
+        // two adjacent lines per 16-byte copy, which bypasses L1 (cp.async.cg) and so leaves the
+        // solve tables resident there
+        int const p = tid % (TL / 2);
+        int const c2 = tid / (TL / 2);
+        int64_t const line = (int64_t)blockIdx.x * TL + 2 * p;
+        bool const live0 = line < args.nlines, live1 = line + 1 < args.nlines;
+        int64_t const ov = live0 ? line_offset(args.lv, line) : 0;
+        for (int r = c2; r < n; r += 2 * nct) {
+            int sr = r + R.lrot;
+            sr -= (sr >= n) ? n : 0;
+            double* dst = T + r * TL + 2 * p;
+            if (sr >= v0 && sr < v1) {
+                if (live1) {
+                    cp_async16(dst, args.vals + (int64_t)(sr - v0) * args.lv.stride + ov);
+                } else {
+                    dst[0] = live0 ? args.vals[(int64_t)(sr - v0) * args.lv.stride + ov] : 0.0;
+                    dst[1] = 0.0;
+                }
+            } else {
+                dst[0] = live0 ? other_row(sr, line) : 0.0;
+                dst[1] = live1 ? other_row(sr, line + 1) : 0.0;
+            }
+        }
+    } else {
+        int const l = tid % TL;
+        int const c = tid / TL;
+        int64_t const line = (int64_t)blockIdx.x * TL + l;
+        bool const live = line < args.nlines;
         int64_t const ov = live ? line_offset(args.lv, line) : 0;
-        int const v0 = (args.raw || R.periodic) ? 0 : R.nbe_lo;
-        int const v1 = (args.raw || R.periodic) ? n : R.nbe_lo + R.npoints;
         for (int r = c; r < n; r += nct) {
             int sr = r + R.lrot;
             sr -= (sr >= n) ? n : 0;
-            if (live && sr >= v0 && sr < v1) {
-                cp_async8(T + r * TL + l, args.vals + (int64_t)(sr - v0) * args.lv.stride + ov);
-            } else {
-                double v = 0.0;
-                if (live && sr < R.nbe_lo) {
-                    if (sr < R.nbv_lo) v = args.dlo[sr * args.llo.stride + line_offset(args.llo, line)] * R.dxpow_lo[sr];
-                } else if (live && sr >= v1) {
-                    int const i = sr - (n - R.nbe_hi);
-                    if (i < R.nbv_hi) v = args.dhi[i * args.lhi.stride + line_offset(args.lhi, line)] * R.dxpow_hi[i];
-                }
-                T[r * TL + l] = v;
-            }
+            if (live && sr >= v0 && sr < v1) cp_async8(T + r * TL + l, args.vals + (int64_t)(sr - v0) * args.lv.stride + ov);
+            else T[r * TL + l] = live && !(sr >= v0 && sr < v1) ? other_row(sr, line) : 0.0;
         }
-        cp_async_wait_all();
     }
+    cp_async_wait_all();
     __syncthreads();
 }
 
 // Steps 2-4 of a solve on a tile already in shared memory (T[j*TL + l] = right-hand side row j of
-// line l): forward and backward sweeps, border correction. On return (after a barrier) T holds the
-// solution. Every thread of the block must call it.
+// line l): forward and backward sweeps, border correction. A thread owns one chunk of a pair of
+// lines (16-byte shared-memory accesses; each factor load serves both lines). On return (after a
+// barrier) T holds the solution. Every thread of the block must call it; TL is even and the block
+// has at least nchunk * TL / 2 threads.
 template <int TL, int KL, int KU>
-__device__ __forceinline__ void solve_in_tile(SolveTables const& t, int nct, double* smem)
+__device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/, double* smem)
 {
+    static_assert(TL % 2 == 0, "the solve works on line pairs");
+    constexpr int P = TL / 2;
     constexpr int KC = KL > KU ? KL : KU;
     int const n = t.n, m = t.m, k = t.k;
     int const NC = t.nchunk;
-    double* T = smem;                              // n x TL
-    double* carry = T + (size_t)n * TL;            // NC x KC x TL
-    double* halo = carry + (size_t)NC * KC * TL;   // NC x KL x TL
-    double* btmp = halo + (size_t)NC * KL * TL;    // k x TL
     int const tid = threadIdx.x;
-    int const l = tid % TL;
-    int const c = tid / TL;
+    int const p = tid % P;
+    int const c = tid / P;
+    int const nthr = blockDim.x / P;                         // threads per pair
+    double2* const T2 = reinterpret_cast<double2*>(smem) + p;  // n rows, stride P
+    double2* const carry = T2 + (size_t)n * P;                // NC x KC rows
+    double2* const halo = carry + (size_t)NC * KC * P;       // NC x KL rows
+    double2* const btmp = halo + (size_t)NC * KL * P;        // k rows
+    double2 const zero = make_double2(0.0, 0.0);
 
     int a = 0, e = 0;
     if (c < NC) {
@@ -212,72 +270,78 @@ __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int nct, dou
     // ---- 2. forward sweep with L (and the row interchanges) ----
     if (m > 0) {
         if (c < NC) {
-            double w[KL + 1];
+            double2 w[KL + 1];
 #pragma unroll
-            for (int q = 0; q < KL; ++q) w[q] = (a + q < m) ? T[(a + q) * TL + l] : 0.0;
-            if (t.pivot) fwd_sweep<KL, true>(t, T, TL, l, a, e, w, false, nullptr, 0);
-            else fwd_sweep<KL, false>(t, T, TL, l, a, e, w, false, nullptr, 0);
+            for (int q = 0; q < KL; ++q) w[q] = (a + q < m) ? T2[(a + q) * P] : zero;
+            if (t.pivot) fwd_sweep<KL, true, false>(t, T2, P, a, e, w, nullptr, 0);
+            else fwd_sweep<KL, false, false>(t, T2, P, a, e, w, nullptr, 0);
 #pragma unroll
             for (int q = 0; q < KL; ++q) {
-                double const orig = (e + q < m) ? T[(e + q) * TL + l] : 0.0;
-                carry[(c * KC + q) * TL + l] = w[q] - orig;
-                halo[(c * KL + q) * TL + l] = orig;
+                double2 const orig = (e + q < m) ? T2[(e + q) * P] : zero;
+                carry[(c * KC + q) * P] = make_double2(w[q].x - orig.x, w[q].y - orig.y);
+                if (t.pivot) halo[(c * KL + q) * P] = orig;
             }
         }
         __syncthreads();
-        carry_scan<KL, KC, TL, true>(t.PhiF, carry, t.nscan, NC, c, l);
+        carry_scan<KL, KC, true>(t.PhiF, carry, P, t.nscan, NC, c);
         if (c < NC) {
-            double w[KL + 1];
+            double2 w[KL + 1];
 #pragma unroll
-            for (int q = 0; q < KL; ++q)
-                w[q] = (a + q < m) ? T[(a + q) * TL + l] + (c > 0 ? carry[((c - 1) * KC + q) * TL + l] : 0.0) : 0.0;
-            if (t.pivot) fwd_sweep<KL, true>(t, T, TL, l, a, e, w, true, halo + (size_t)c * KL * TL + l, TL);
-            else fwd_sweep<KL, false>(t, T, TL, l, a, e, w, true, halo + (size_t)c * KL * TL + l, TL);
+            for (int q = 0; q < KL; ++q) {
+                double2 v = (a + q < m) ? T2[(a + q) * P] : zero;
+                if (c > 0 && a + q < m) {
+                    double2 const cin = carry[((c - 1) * KC + q) * P];
+                    v.x += cin.x;
+                    v.y += cin.y;
+                }
+                w[q] = v;
+            }
+            if (t.pivot) fwd_sweep<KL, true, true>(t, T2, P, a, e, w, halo + (size_t)c * KL * P, P);
+            else fwd_sweep<KL, false, true>(t, T2, P, a, e, w, nullptr, 0);
         }
         __syncthreads();
 
         // ---- 3. backward sweep with U ----
         if (c < NC) {
-            double z[KU];
+            double2 z[KU];
 #pragma unroll
-            for (int q = 0; q < KU; ++q) z[q] = 0.0;
-            bwd_sweep<KU>(t, T, TL, l, a, e, z, false);
+            for (int q = 0; q < KU; ++q) z[q] = zero;
+            bwd_sweep<KU, false>(t, T2, P, a, e, z);
 #pragma unroll
-            for (int q = 0; q < KU; ++q) carry[(c * KC + q) * TL + l] = z[q];
+            for (int q = 0; q < KU; ++q) carry[(c * KC + q) * P] = z[q];
         }
         __syncthreads();
-        carry_scan<KU, KC, TL, false>(t.PhiB, carry, t.nscan, NC, c, l);
+        carry_scan<KU, KC, false>(t.PhiB, carry, P, t.nscan, NC, c);
         if (c < NC) {
-            double z[KU];
+            double2 z[KU];
 #pragma unroll
-            for (int q = 0; q < KU; ++q) z[q] = (c + 1 < NC) ? carry[((c + 1) * KC + q) * TL + l] : 0.0;
-            bwd_sweep<KU>(t, T, TL, l, a, e, z, true);
+            for (int q = 0; q < KU; ++q) z[q] = (c + 1 < NC) ? carry[((c + 1) * KC + q) * P] : zero;
+            bwd_sweep<KU, true>(t, T2, P, a, e, z);
         }
         __syncthreads();
     }
 
     // ---- 4. border: x2 = S^-1 (b2 - lambda x'), x1 = x' - (Q^-1 gamma) x2 ----
     if (k > 0) {
-        // border row r is handled by chunk thread r of the line
-        for (int r = c; r < k; r += nct) {
-            double s = T[(m + r) * TL + l];
+        for (int r = c; r < k; r += nthr) {
+            double2 s = T2[(m + r) * P];
             int const q1 = __ldg(t.lam_row + r + 1);
-            for (int q = __ldg(t.lam_row + r); q < q1; ++q) s = fma(-__ldg(t.lam_val + q), T[__ldg(t.lam_col + q) * TL + l], s);
-            btmp[r * TL + l] = s;
+            for (int q = __ldg(t.lam_row + r); q < q1; ++q) s = fma2(-__ldg(t.lam_val + q), T2[__ldg(t.lam_col + q) * P], s);
+            btmp[r * P] = s;
         }
         __syncthreads();
-        for (int r = c; r < k; r += nct) {
-            double s = 0.0;
-            for (int q = 0; q < k; ++q) s = fma(__ldg(t.Sinv + r * k + q), btmp[q * TL + l], s);
-            T[(m + r) * TL + l] = s;
+        for (int r = c; r < k; r += nthr) {
+            double2 s = zero;
+            for (int q = 0; q < k; ++q) s = fma2(__ldg(t.Sinv + r * k + q), btmp[q * P], s);
+            T2[(m + r) * P] = s;
         }
         __syncthreads();
         int const nq = t.qg_lo + t.qg_hi;
-        for (int q = c; q < nq; q += nct) {
+        for (int q = c; q < nq; q += nthr) {
             int const i = q < t.qg_lo ? q : m - t.qg_hi + (q - t.qg_lo);
-            double s = T[i * TL + l];
-            for (int r = 0; r < k; ++r) s = fma(-__ldg(t.Qg + (size_t)q * k + r), T[(m + r) * TL + l], s);
-            T[i * TL + l] = s;
+            double2 s = T2[i * P];
+            for (int r = 0; r < k; ++r) s = fma2(-__ldg(t.Qg + (size_t)q * k + r), T2[(m + r) * P], s);
+            T2[i * P] = s;
         }
         __syncthreads();
     }
@@ -303,19 +367,35 @@ __device__ __forceinline__ int coef_row(RhsMap const& R, int n, int b)
     return r;
 }
 
-// Step 5: store the coefficients of the tile.
+// Step 5: store the coefficients of the tile (streaming stores: the output is not read again by
+// this kernel).
 template <int TL>
 __device__ __forceinline__ void store_tile(BuildArgs const& args, const double* T)
 {
     int const n = args.t.n;
     int const tid = threadIdx.x;
+    int const rows = args.raw ? n : args.r.size;
+    if (TL % 2 == 0 && args.pair16_out) {
+        int const p = tid % (TL / 2);
+        int const c2 = tid / (TL / 2);
+        int64_t const line = (int64_t)blockIdx.x * TL + 2 * p;
+        if (line >= args.nlines) return;
+        int64_t const oo = line_offset(args.lo, line);
+        bool const live1 = line + 1 < args.nlines;
+        for (int r = c2; r < rows; r += 2 * args.nct) {
+            double2 const v = *reinterpret_cast<const double2*>(T + coef_row(args.r, n, r) * TL + 2 * p);
+            double* dst = args.out + r * args.lo.stride + oo;
+            if (live1) __stcs(reinterpret_cast<double2*>(dst), v);
+            else __stcs(dst, v.x);
+        }
+        return;
+    }
     int const l = tid % TL;
     int const c = tid / TL;
     int64_t const line = (int64_t)blockIdx.x * TL + l;
     if (line >= args.nlines) return;
     int64_t const oo = line_offset(args.lo, line);
-    int const rows = args.raw ? n : args.r.size;
-    for (int r = c; r < rows; r += args.nct) args.out[r * args.lo.stride + oo] = T[coef_row(args.r, n, r) * TL + l];
+    for (int r = c; r < rows; r += args.nct) __stcs(args.out + r * args.lo.stride + oo, T[coef_row(args.r, n, r) * TL + l]);
 }
 
 } // namespace ddcb

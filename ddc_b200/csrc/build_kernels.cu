@@ -41,10 +41,10 @@ template <int KL, int KU>
 void launch_k(BuildArgs const& args, int TL, cudaStream_t s)
 {
     switch (TL) {
-    case 1: launch_tl<1, KL, KU>(args, s); break;
+    case 2: launch_tl<2, KL, KU>(args, s); break;
     case 4: launch_tl<4, KL, KU>(args, s); break;
     case 8: launch_tl<8, KL, KU>(args, s); break;
-    default: throw Error(DDCB_ERR_UNSUPPORTED, "tile_lines must be 1, 4 or 8");
+    default: throw Error(DDCB_ERR_UNSUPPORTED, "tile_lines must be 2, 4 or 8");
     }
 }
 
@@ -68,13 +68,14 @@ void dispatch(BuildArgs const& args, int TL, cudaStream_t s)
 
 int pick_nct(SolveTables const& t, int TL)
 {
-    // chunk threads per line: enough for the sweeps, a multiple of 32/TL, 128..1024 threads
-    int nct = std::max(t.nchunk, 1);
-    int const warp_mult = std::max(1, 32 / TL);
-    nct = (nct + warp_mult - 1) / warp_mult * warp_mult;
-    while (nct * TL < 128) nct += warp_mult;
-    while (nct * TL > 1024) nct -= warp_mult;
-    return nct;
+    // threads per line pair: one per chunk, rounded so the block is whole warps (at least two);
+    // returned as threads per line (block = TL * nct)
+    int const P = TL / 2;
+    int const mult = std::max(1, 32 / P);
+    int nthr = (std::max(t.nchunk, 1) + mult - 1) / mult * mult;
+    while (P * nthr < 64) nthr += mult;
+    while (P * nthr > 1024) nthr -= mult;
+    return nthr / 2;
 }
 
 } // namespace
@@ -100,6 +101,8 @@ BuildArgs make_build_args(Builder const& b, double* coefs, Lines const& lc, doub
     args.out = coefs;
     args.lo = lc;
     args.nct = pick_nct(b.tables, b.tile_lines);
+    args.pair16 = line_pairs_aligned(vals, lv);
+    args.pair16_out = line_pairs_aligned(coefs, lc);
     return args;
 }
 } // namespace
@@ -140,6 +143,8 @@ void launch_build(Builder const& b, double* coefs, Lines const& lc, double const
     args.out = coefs;
     args.lo = lc;
     args.nct = pick_nct(b.tables, b.tile_lines);
+    args.pair16 = line_pairs_aligned(vals, lv);
+    args.pair16_out = line_pairs_aligned(coefs, lc);
     if (args.nlines == 0) return;
     dispatch(args, b.tile_lines, s);
 }
@@ -161,6 +166,7 @@ void launch_solve_multirhs(Builder const& b, double* rhs, long ld, long nrhs, bo
     args.out = rhs;
     args.lo = L;
     args.nct = pick_nct(args.t, b.tile_lines);
+    args.pair16 = args.pair16_out = line_pairs_aligned(rhs, L);
     if (nrhs == 0) return;
     dispatch(args, b.tile_lines, s);
 }

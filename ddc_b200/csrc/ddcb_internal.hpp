@@ -37,6 +37,14 @@ struct Lines
 
 inline Lines to_lines(ddcb_lines const& l) { return Lines {l.n, l.stride, l.inner, l.outer, l.outer_stride}; }
 
+// Whether lines (2i, 2i+1) of a layout sit side by side at 16-byte aligned addresses, so a tile
+// can move two lines per 16-byte copy.
+inline bool line_pairs_aligned(const void* base, Lines const& L)
+{
+    return (reinterpret_cast<uintptr_t>(base) % 16 == 0) && L.stride % 2 == 0 && L.inner % 2 == 0
+           && (L.outer <= 1 || L.outer_stride % 2 == 0);
+}
+
 // Device-side description of the banded solve of one builder (all pointers are device pointers).
 //
 // The system A (size n) is split as [[Q, g],[l, S0]] with a border of k rows/cols (periodic corner
@@ -51,6 +59,8 @@ struct SolveTables
     int nchunk;      // chunks per line used by the sweeps
     int chunk_len;   // every chunk but the last has this (odd) length; the last absorbs the rest
     int nscan;       // steps of the log-depth carry scan: ceil(log2(nchunk))
+    int cj0, cj1, cshift; // rows [cj0, cj1) of Lf / piv / Uf are identical and stored once (at
+                          // cj0); later rows move up by cshift = cj1 - cj0 - 1 (0: no run)
     const double* Lf;    // m x kl: Lf[j*kl + t-1] = multiplier of row j+t at step j
     const int8_t* piv;   // m: pivot row offset at step j (ipiv[j] - j)
     const double* Uf;    // m x (ku+1): [1/U_jj, U_j,j+1 .. U_j,j+ku]

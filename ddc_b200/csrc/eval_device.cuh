@@ -59,6 +59,16 @@ struct CoefRotated
     }
 };
 
+// CoefGlobal: coefficients in basis order in global memory (row b at C[b*cs]), read through the
+// read-only cache.
+struct CoefGlobal
+{
+    const double* C;
+    int64_t cs;
+    __device__ __forceinline__ int row0(int jmin) const { return jmin; }
+    __device__ __forceinline__ double get(int r0, int i) const { return __ldg(C + (int64_t)(r0 + i) * cs); }
+};
+
 // Cell of x as a knot index (the cell [t_c, t_c+1) with t_c <= x < t_c+1), with the end rules of
 // bsplines_non_uniform.hpp:666-695. A bucket table gives a starting cell; short walks finish it,
 // so the result equals the bisection's for any mesh.

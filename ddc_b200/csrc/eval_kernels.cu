@@ -29,6 +29,7 @@ struct EvalArgs
     Lines lc;
     double* out;
     Lines lo;
+    int pair16;         // coefs: adjacent line pairs 16-byte aligned and contiguous
 };
 
 __device__ __forceinline__ int64_t line_offset(Lines const& L, int64_t b)
@@ -62,7 +63,19 @@ __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const __grid_constan
     int const nct = blockDim.x / TLE;
     int64_t const line = (int64_t)blockIdx.x * TLE + l;
     bool const live = line < a.nlines;
-    if (live) {
+    if (a.pair16) {
+        // two lines per 16-byte copy (cp.async.cg bypasses L1, where the basis tables live)
+        int const p = tid % (TLE / 2);
+        int const c2 = tid / (TLE / 2);
+        int64_t const l0 = (int64_t)blockIdx.x * TLE + 2 * p;
+        if (l0 + 1 < a.nlines) {
+            int64_t const oc = line_offset(a.lc, l0);
+            for (int r = c2; r < a.size; r += 2 * nct) cp_async16(C + r * TLE + 2 * p, a.coefs + r * a.lc.stride + oc);
+        } else if (l0 < a.nlines) {
+            int64_t const oc = line_offset(a.lc, l0);
+            for (int r = c2; r < a.size; r += 2 * nct) cp_async8(C + r * TLE + 2 * p, a.coefs + r * a.lc.stride + oc);
+        }
+    } else if (live) {
         int64_t const oc = line_offset(a.lc, line);
         for (int r = c; r < a.size; r += nct) cp_async8(C + r * TLE + l, a.coefs + r * a.lc.stride + oc);
     }
@@ -85,10 +98,10 @@ __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const __grid_constan
     for (int q0 = 0; q0 < npt; q0 += U) {
         double xs[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) xs[u] = (q0 + u < npt) ? xp[(q0 + u) * sx] : 0.0;
+        for (int u = 0; u < U; ++u) xs[u] = (q0 + u < npt) ? __ldcs(xp + (q0 + u) * sx) : 0.0;
 #pragma unroll
         for (int u = 0; u < U; ++u)
-            if (q0 + u < npt) op[(q0 + u) * so] = eval_point<D, ORDER, UNI>(eb, a.ex_lo, a.ex_hi, xs[u], acc);
+            if (q0 + u < npt) __stcs(op + (q0 + u) * so, eval_point<D, ORDER, UNI>(eb, a.ex_lo, a.ex_hi, xs[u], acc));
     }
 }
 
@@ -159,6 +172,7 @@ void launch_eval(Evaluator const& e, int order, double* out, Lines const& lo, do
     a.lc = lc;
     a.out = out;
     a.lo = lo;
+    a.pair16 = line_pairs_aligned(coefs, lc);
     if (a.nlines == 0 || lx.n == 0) return;
     constexpr int TLE = 8;
     size_t sm = sizeof(double) * ((size_t)a.size * TLE + (e.eb.b.uniform ? 0 : 2 * (size_t)e.eb.nk));

@@ -54,10 +54,10 @@ __global__ void __launch_bounds__(1024) build_eval_kernel(const __grid_constant_
     for (int q0 = 0; q0 < npt; q0 += U) {
         double xs[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) xs[u] = (q0 + u < npt) ? xp[(q0 + u) * sx] : 0.0;
+        for (int u = 0; u < U; ++u) xs[u] = (q0 + u < npt) ? __ldcs(xp + (q0 + u) * sx) : 0.0;
 #pragma unroll
         for (int u = 0; u < U; ++u)
-            if (q0 + u < npt) op[(q0 + u) * so] = eval_point<D, ORDER, UNI>(eb, fe.ex_lo, fe.ex_hi, xs[u], acc);
+            if (q0 + u < npt) __stcs(op + (q0 + u) * so, eval_point<D, ORDER, UNI>(eb, fe.ex_lo, fe.ex_hi, xs[u], acc));
     }
 }
 

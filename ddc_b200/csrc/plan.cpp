@@ -719,9 +719,38 @@ SolveTables upload_tables(HostSolve const& h, std::vector<char>& blob, std::vect
         offs.push_back(off);
         return off;
     };
-    push(h.Lf.data(), h.Lf.size() * 8);
-    push(h.piv.data(), h.piv.size());
-    push(h.Uf.data(), h.Uf.size() * 8);
+    // The longest run of identical factor rows (the steady state a constant-coefficient band
+    // reaches after a few rows) is stored once, so the tables of uniform meshes stay L1-resident.
+    long const m = h.m, kl = h.kl, ku1 = h.ku + 1;
+    auto same_row = [&](long i, long j) {
+        return std::memcmp(&h.Lf[i * kl], &h.Lf[j * kl], sizeof(double) * kl) == 0
+               && std::memcmp(&h.Uf[i * ku1], &h.Uf[j * ku1], sizeof(double) * ku1) == 0 && h.piv[i] == h.piv[j];
+    };
+    long best0 = m, best1 = m;
+    for (long i = 0; i < m;) {
+        long j = i + 1;
+        while (j < m && same_row(i, j)) ++j;
+        if (j - i > best1 - best0) {
+            best0 = i;
+            best1 = j;
+        }
+        i = j;
+    }
+    if (best1 - best0 < 8) best0 = best1 = m;
+    t.cj0 = int(best0);
+    t.cj1 = int(best1);
+    t.cshift = best1 > best0 ? int(best1 - best0 - 1) : 0;
+    std::vector<double> Lc, Uc;
+    std::vector<int8_t> pc;
+    for (long j = 0; j < m; ++j) {
+        if (j > best0 && j < best1) continue;
+        Lc.insert(Lc.end(), h.Lf.begin() + j * kl, h.Lf.begin() + (j + 1) * kl);
+        Uc.insert(Uc.end(), h.Uf.begin() + j * ku1, h.Uf.begin() + (j + 1) * ku1);
+        pc.push_back(h.piv[j]);
+    }
+    push(Lc.data(), Lc.size() * 8);
+    push(pc.data(), pc.size());
+    push(Uc.data(), Uc.size() * 8);
     push(h.PhiF.data(), h.PhiF.size() * 8);
     push(h.PhiB.data(), h.PhiB.size() * 8);
     push(h.lam_row.data(), h.lam_row.size() * 4);
@@ -825,8 +854,8 @@ Builder* create_builder_host(Basis const& basis, double const* pts, long npts, i
             if (opts->tile_lines > 0) b->tile_lines = opts->tile_lines;
             if (opts->chunks > 0) b->nchunk_req = opts->chunks;
         }
-        if (b->tile_lines != 1 && b->tile_lines != 4 && b->tile_lines != 8)
-            throw Error(DDCB_ERR_INVALID_ARGUMENT, "tile_lines must be 1, 4 or 8");
+        if (b->tile_lines != 2 && b->tile_lines != 4 && b->tile_lines != 8)
+            throw Error(DDCB_ERR_INVALID_ARGUMENT, "tile_lines must be 2, 4 or 8");
         if (b->nchunk_req * b->tile_lines > 1024) throw Error(DDCB_ERR_INVALID_ARGUMENT, "tile_lines*chunks must be <= 1024");
         check_valid_grid(*b);
         // compute_offset (spline_builder.hpp:619-658)
