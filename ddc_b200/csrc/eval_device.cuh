@@ -16,7 +16,8 @@ struct EvalBasis
 {
     BasisDesc b;              // b.knots: device knots
     const double2* kpairs;    // nk-1 pairs (t_i, t_i+1): device copy, or shared-memory copy in a kernel
-    const double* inv_span;   // degree x nk: inv_span[(len-1)*nk + i] = 1/(t[i+len] - t[i]) (0 if empty)
+    const double* inv_span;   // degree x nk: inv_span[(len-1)*nk + i] = 1/(t[i+len] - t[i]) (0 if empty);
+                              // global memory, or a shared-memory copy in a kernel (plain loads)
     const int* lut;           // nbucket entries: knot index of the cell holding each bucket start
     int nbucket;
     double bucket_scale;      // nbucket / (rmax - rmin)
@@ -114,7 +115,7 @@ __device__ __forceinline__ void nonuniform_values_span(const double* kn, const d
         double saved = 0.0;
 #pragma unroll
         for (int r = 0; r < j + 1; ++r) {
-            double const temp = v[r] * __ldg(ispan + j * nk + r - j);
+            double const temp = v[r] * ispan[j * nk + r - j];
             v[r] = saved + right[r] * temp;
             saved = left[j - r] * temp;
         }
@@ -138,7 +139,7 @@ __device__ __forceinline__ void nonuniform_values_span2(const double* kn, const 
         double saved = 0.0;
 #pragma unroll
         for (int r = 0; r < j + 1; ++r) {
-            double const temp = v[r] * __ldg(ispan + j * nk + r - j);
+            double const temp = v[r] * ispan[j * nk + r - j];
             v[r] = saved + right[r] * temp;
             saved = left[j - r] * temp;
         }
@@ -228,7 +229,7 @@ __device__ __forceinline__ double eval_deriv_no_bc(EvalBasis const& eb, double x
 #pragma unroll
         for (int i = D; i >= k; --i) {
             if (UNI) cc[i] = (cc[i] - cc[i - 1]) * eb.b.inv_step;
-            else cc[i] = double(D - k + 1) * (cc[i] - cc[i - 1]) * __ldg(dspan + (D - k) * eb.nk + i);
+            else cc[i] = double(D - k + 1) * (cc[i] - cc[i - 1]) * dspan[(D - k) * eb.nk + i];
         }
     }
     double y = 0.0;
@@ -297,8 +298,8 @@ __device__ __forceinline__ int basis_derivs(EvalBasis const& eb, double x, doubl
                 fb = eb.b.inv_step;
             } else {
                 int const p = D - k + 1;
-                fa = double(p) * __ldg(eb.inv_span + (p - 1) * eb.nk + jmin + i);
-                fb = double(p) * __ldg(eb.inv_span + (p - 1) * eb.nk + jmin + i + 1);
+                fa = double(p) * eb.inv_span[(p - 1) * eb.nk + jmin + i];
+                fb = double(p) * eb.inv_span[(p - 1) * eb.nk + jmin + i + 1];
             }
             nw[i] = fa * a - fb * ((i + 1 <= D && i + 1 >= k) ? b : 0.0);
         }
@@ -355,7 +356,7 @@ __device__ __forceinline__ int point_adjoint(EvalBasis const& eb, int ex_lo, int
 #pragma unroll
             for (int i = 1; i <= D; ++i) {
                 double const ci = C.get(r0, i);
-                double const f = UNI ? eb.b.inv_step : double(D) * __ldg(eb.inv_span + (D - 1) * eb.nk + jmin + i);
+                double const f = UNI ? eb.b.inv_step : double(D) * eb.inv_span[(D - 1) * eb.nk + jmin + i];
                 y = fma((ci - cprev) * f, vp[i - 1], y);
                 cprev = ci;
             }
