@@ -59,12 +59,6 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
 
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// Shared-memory doubles of one tile: the rows, the carries, the halo rows and the border scratch.
-__host__ __device__ inline size_t tile_doubles(SolveTables const& t, int TL, int KL, int KU)
-{
-    int const KC = KL > KU ? KL : KU;
-    return (size_t)t.n * TL + (size_t)t.nchunk * KC * TL + (size_t)t.nchunk * KL * TL + (size_t)t.k * TL;
-}
 
 // Row of the factor tables holding row j: runs of identical rows (the steady state of a
 // constant-coefficient band) are stored once (plan.cpp, upload_tables).
@@ -77,21 +71,61 @@ __device__ __forceinline__ double2 fma2(double a, double2 y, double2 w)
 {
     return make_double2(fma(a, y.x, w.x), fma(a, y.y, w.y));
 }
+__device__ __forceinline__ float2 fma2(float a, float2 y, float2 w) { return make_float2(fmaf(a, y.x, w.x), fmaf(a, y.y, w.y)); }
+__device__ __forceinline__ double2 mul2(double2 v, double d) { return make_double2(v.x * d, v.y * d); }
+__device__ __forceinline__ float2 mul2(float2 v, float d) { return make_float2(v.x * d, v.y * d); }
+__device__ __forceinline__ double2 add2(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 sub2(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
+// The factor tables in the arithmetic type R of a solve: the FP64 tables, or their FP32 copies
+// (the FP32 solves of the refinement mode).
+template <class R>
+struct Fac;
+template <>
+struct Fac<double>
+{
+    using V = double2;
+    __device__ static V zero() { return make_double2(0.0, 0.0); }
+    __device__ static const double* Lf(SolveTables const& t) { return t.Lf; }
+    __device__ static const double* Uf(SolveTables const& t) { return t.Uf; }
+    __device__ static const double* PhiF(SolveTables const& t) { return t.PhiF; }
+    __device__ static const double* PhiB(SolveTables const& t) { return t.PhiB; }
+    __device__ static const double* lam(SolveTables const& t) { return t.lam_val; }
+    __device__ static const double* Sinv(SolveTables const& t) { return t.Sinv; }
+    __device__ static const double* Qg(SolveTables const& t) { return t.Qg; }
+};
+template <>
+struct Fac<float>
+{
+    using V = float2;
+    __device__ static V zero() { return make_float2(0.f, 0.f); }
+    __device__ static const float* Lf(SolveTables const& t) { return t.f32.Lf; }
+    __device__ static const float* Uf(SolveTables const& t) { return t.f32.Uf; }
+    __device__ static const float* PhiF(SolveTables const& t) { return t.f32.PhiF; }
+    __device__ static const float* PhiB(SolveTables const& t) { return t.f32.PhiB; }
+    __device__ static const float* lam(SolveTables const& t) { return t.f32.lam_val; }
+    __device__ static const float* Sinv(SolveTables const& t) { return t.f32.Sinv; }
+    __device__ static const float* Qg(SolveTables const& t) { return t.f32.Qg; }
+};
 
 // Forward sweep with L (and the row interchanges when PIV) over rows [a, e) of a line pair; T2
 // points at the pair's column (row j at T2[j*P]). w[0..KL-1] hold rows a..a+KL-1 on entry. Phase A
 // (WRITE false) reads rows beyond e from the tile, which nothing has written yet. Phase C (WRITE
 // true) writes rows a..e-1; without interchanges rows beyond e only feed the next chunk's rows,
 // so they are not read; with interchanges they come from the halo copy.
-template <int KL, bool PIV, bool WRITE>
-__device__ __forceinline__ void fwd_sweep(SolveTables const& t, double2* T2, int P, int a, int e, double2* w,
-                                          const double2* halo, int hstride)
+template <class R, int KL, bool PIV, bool WRITE>
+__device__ __forceinline__ void fwd_sweep(SolveTables const& t, typename Fac<R>::V* T2, int P, int a, int e,
+                                          typename Fac<R>::V* w, const typename Fac<R>::V* halo, int hstride)
 {
+    using V = typename Fac<R>::V;
+    R const* __restrict__ Lf = Fac<R>::Lf(t);
     int const lim = (WRITE && !PIV) ? e : t.m; // fill rows below lim are read
 #pragma unroll 4
     for (int j = a; j < e; ++j) {
         int const rr = j + KL;
-        double2 fill = make_double2(0.0, 0.0);
+        V fill = Fac<R>::zero();
         if (rr < e) fill = T2[rr * P];
         else if (rr < lim) fill = (WRITE && PIV) ? halo[(rr - e) * hstride] : T2[rr * P];
         w[KL] = fill;
@@ -101,14 +135,14 @@ __device__ __forceinline__ void fwd_sweep(SolveTables const& t, double2* T2, int
 #pragma unroll
             for (int q = 1; q <= KL; ++q)
                 if (pv == q) {
-                    double2 const s = w[0];
+                    V const s = w[0];
                     w[0] = w[q];
                     w[q] = s;
                 }
         }
-        double2 const y = w[0];
+        V const y = w[0];
         if (WRITE) T2[j * P] = y;
-        double const* L = t.Lf + (size_t)cj * KL;
+        R const* L = Lf + (size_t)cj * KL;
 #pragma unroll
         for (int q = 1; q <= KL; ++q) w[q] = fma2(-__ldg(L + q - 1), y, w[q]);
 #pragma unroll
@@ -118,17 +152,19 @@ __device__ __forceinline__ void fwd_sweep(SolveTables const& t, double2* T2, int
 
 // Backward sweep with U over rows e-1 .. a of a line pair; z[0..KU-1] hold the solution rows
 // e .. e+KU-1 (the carry from the chunk below) on entry.
-template <int KU, bool WRITE>
-__device__ __forceinline__ void bwd_sweep(SolveTables const& t, double2* T2, int P, int a, int e, double2* z)
+template <class R, int KU, bool WRITE>
+__device__ __forceinline__ void bwd_sweep(SolveTables const& t, typename Fac<R>::V* T2, int P, int a, int e,
+                                          typename Fac<R>::V* z)
 {
+    using V = typename Fac<R>::V;
+    R const* __restrict__ Uf = Fac<R>::Uf(t);
 #pragma unroll 4
     for (int j = e - 1; j >= a; --j) {
-        double const* U = t.Uf + (size_t)crow(t, j) * (KU + 1);
-        double2 s = T2[j * P];
+        R const* U = Uf + (size_t)crow(t, j) * (KU + 1);
+        V s = T2[j * P];
 #pragma unroll
         for (int q = 1; q <= KU; ++q) s = fma2(-__ldg(U + q), z[q - 1], s);
-        double const d = __ldg(U);
-        double2 const x = make_double2(s.x * d, s.y * d);
+        V const x = mul2(s, __ldg(U));
         if (WRITE) T2[j * P] = x;
 #pragma unroll
         for (int q = KU - 1; q >= 1; --q) z[q] = z[q - 1];
@@ -142,10 +178,12 @@ __device__ __forceinline__ void bwd_sweep(SolveTables const& t, double2* T2, int
 // out(c) = Phi_c out(c-1) + hat(c); step k adds P(k,c) y(c-2^k). Backward: the carry flows from
 // c+1 into c with Q(k,c) y(c+2^k). Every thread of the block takes part in the barriers; threads
 // of chunk c < NC do the arithmetic.
-template <int K, int KC, bool FWD>
-__device__ __forceinline__ void carry_scan(const double* __restrict__ Pm, double2* C2, int P, int nscan, int NC, int c)
+template <class R, int K, int KC, bool FWD>
+__device__ __forceinline__ void carry_scan(const R* __restrict__ Pm, typename Fac<R>::V* C2, int P, int nscan, int NC,
+                                           int c)
 {
-    double2 y[K];
+    using V = typename Fac<R>::V;
+    V y[K];
     bool const act = c < NC;
     if (act) {
 #pragma unroll
@@ -154,17 +192,17 @@ __device__ __forceinline__ void carry_scan(const double* __restrict__ Pm, double
     for (int k = 0; k < nscan; ++k) {
         int const nb = FWD ? c - (1 << k) : c + (1 << k);
         bool const has = act && (FWD ? nb >= 0 : nb < NC);
-        double2 v[K];
+        V v[K];
         if (has) {
 #pragma unroll
             for (int q = 0; q < K; ++q) v[q] = C2[(nb * KC + q) * P];
         }
         __syncthreads();
         if (has) {
-            double const* M = Pm + ((size_t)k * NC + c) * K * K;
+            R const* M = Pm + ((size_t)k * NC + c) * K * K;
 #pragma unroll
             for (int r = 0; r < K; ++r) {
-                double2 s = y[r];
+                V s = y[r];
 #pragma unroll
                 for (int q = 0; q < K; ++q) s = fma2(__ldg(M + r * K + q), v[q], s);
                 y[r] = s;
@@ -174,6 +212,139 @@ __device__ __forceinline__ void carry_scan(const double* __restrict__ Pm, double
         }
         __syncthreads();
     }
+}
+
+// Shared-memory doubles of one tile: the rows, the carries, the halo rows and the border scratch.
+__host__ __device__ inline size_t tile_doubles(SolveTables const& t, int TL, int KL, int KU)
+{
+    int const KC = KL > KU ? KL : KU;
+    return (size_t)t.n * TL + (size_t)t.nchunk * KC * TL + (size_t)t.nchunk * KL * TL + (size_t)t.k * TL;
+}
+
+// Steps 2-4 of a solve on a tile already in shared memory (T[j*TL + l] = right-hand side row j of
+// line l, in the arithmetic type R): forward and backward sweeps, border correction. A thread owns
+// one chunk of a pair of lines (paired shared-memory accesses; each factor load serves both
+// lines). The carries, halo and border scratch follow the n rows (tile_doubles elements of R in
+// all). On return (after a barrier) T holds the solution. Every thread of the block must call it;
+// TL is even and the block has at least nchunk * TL / 2 threads.
+template <int TL, int KL, int KU, class R = double>
+__device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/, R* smem)
+{
+    static_assert(TL % 2 == 0, "the solve works on line pairs");
+    using V = typename Fac<R>::V;
+    constexpr int P = TL / 2;
+    constexpr int KC = KL > KU ? KL : KU;
+    int const n = t.n, m = t.m, k = t.k;
+    int const NC = t.nchunk;
+    int const tid = threadIdx.x;
+    int const p = tid % P;
+    int const c = tid / P;
+    int const nthr = blockDim.x / P;                     // threads per pair
+    V* const T2 = reinterpret_cast<V*>(smem) + p;        // n rows, stride P
+    V* const carry = T2 + (size_t)n * P;                 // NC x KC rows
+    V* const halo = carry + (size_t)NC * KC * P;         // NC x KL rows
+    V* const btmp = halo + (size_t)NC * KL * P;          // k rows
+    V const zero = Fac<R>::zero();
+
+    int a = 0, e = 0;
+    if (c < NC) {
+        a = c * t.chunk_len;
+        e = (c == NC - 1) ? m : a + t.chunk_len;
+    }
+
+    // ---- 2. forward sweep with L (and the row interchanges) ----
+    if (m > 0) {
+        if (c < NC) {
+            V w[KL + 1];
+#pragma unroll
+            for (int q = 0; q < KL; ++q) w[q] = (a + q < m) ? T2[(a + q) * P] : zero;
+            if (t.pivot) fwd_sweep<R, KL, true, false>(t, T2, P, a, e, w, nullptr, 0);
+            else fwd_sweep<R, KL, false, false>(t, T2, P, a, e, w, nullptr, 0);
+#pragma unroll
+            for (int q = 0; q < KL; ++q) {
+                V const orig = (e + q < m) ? T2[(e + q) * P] : zero;
+                carry[(c * KC + q) * P] = sub2(w[q], orig);
+                if (t.pivot) halo[(c * KL + q) * P] = orig;
+            }
+        }
+        __syncthreads();
+        carry_scan<R, KL, KC, true>(Fac<R>::PhiF(t), carry, P, t.nscan, NC, c);
+        if (c < NC) {
+            V w[KL + 1];
+#pragma unroll
+            for (int q = 0; q < KL; ++q) {
+                V v = (a + q < m) ? T2[(a + q) * P] : zero;
+                if (c > 0 && a + q < m) v = add2(v, carry[((c - 1) * KC + q) * P]);
+                w[q] = v;
+            }
+            if (t.pivot) fwd_sweep<R, KL, true, true>(t, T2, P, a, e, w, halo + (size_t)c * KL * P, P);
+            else fwd_sweep<R, KL, false, true>(t, T2, P, a, e, w, nullptr, 0);
+        }
+        __syncthreads();
+
+        // ---- 3. backward sweep with U ----
+        if (c < NC) {
+            V z[KU];
+#pragma unroll
+            for (int q = 0; q < KU; ++q) z[q] = zero;
+            bwd_sweep<R, KU, false>(t, T2, P, a, e, z);
+#pragma unroll
+            for (int q = 0; q < KU; ++q) carry[(c * KC + q) * P] = z[q];
+        }
+        __syncthreads();
+        carry_scan<R, KU, KC, false>(Fac<R>::PhiB(t), carry, P, t.nscan, NC, c);
+        if (c < NC) {
+            V z[KU];
+#pragma unroll
+            for (int q = 0; q < KU; ++q) z[q] = (c + 1 < NC) ? carry[((c + 1) * KC + q) * P] : zero;
+            bwd_sweep<R, KU, true>(t, T2, P, a, e, z);
+        }
+        __syncthreads();
+    }
+
+    // ---- 4. border: x2 = S^-1 (b2 - lambda x'), x1 = x' - (Q^-1 gamma) x2 ----
+    if (k > 0) {
+        R const* lam = Fac<R>::lam(t);
+        R const* Sinv = Fac<R>::Sinv(t);
+        R const* Qg = Fac<R>::Qg(t);
+        for (int r = c; r < k; r += nthr) {
+            V s = T2[(m + r) * P];
+            int const q1 = __ldg(t.lam_row + r + 1);
+            for (int q = __ldg(t.lam_row + r); q < q1; ++q) s = fma2(-__ldg(lam + q), T2[__ldg(t.lam_col + q) * P], s);
+            btmp[r * P] = s;
+        }
+        __syncthreads();
+        for (int r = c; r < k; r += nthr) {
+            V s = zero;
+            for (int q = 0; q < k; ++q) s = fma2(__ldg(Sinv + r * k + q), btmp[q * P], s);
+            T2[(m + r) * P] = s;
+        }
+        __syncthreads();
+        int const nq = t.qg_lo + t.qg_hi;
+        for (int q = c; q < nq; q += nthr) {
+            int const i = q < t.qg_lo ? q : m - t.qg_hi + (q - t.qg_lo);
+            V s = T2[i * P];
+            for (int r = 0; r < k; ++r) s = fma2(-__ldg(Qg + (size_t)q * k + r), T2[(m + r) * P], s);
+            T2[i * P] = s;
+        }
+        __syncthreads();
+    }
+}
+
+// Right-hand side value of tile row r of a line (the value the gather below places there): a
+// sample, a dx-scaled Hermite derivative, or 0.
+__device__ __forceinline__ double rhs_row(BuildArgs const& args, int r, int64_t line)
+{
+    RhsMap const& R = args.r;
+    int const n = args.t.n;
+    int const v0 = (args.raw || R.periodic) ? 0 : R.nbe_lo;
+    int const v1 = (args.raw || R.periodic) ? n : R.nbe_lo + R.npoints;
+    int sr = r + R.lrot;
+    sr -= (sr >= n) ? n : 0;
+    if (sr >= v0 && sr < v1) return args.vals[(int64_t)(sr - v0) * args.lv.stride + line_offset(args.lv, line)];
+    if (sr < R.nbe_lo) return sr < R.nbv_lo ? args.dlo[sr * args.llo.stride + line_offset(args.llo, line)] * R.dxpow_lo[sr] : 0.0;
+    int const i = sr - (n - R.nbe_hi);
+    return i < R.nbv_hi ? args.dhi[i * args.lhi.stride + line_offset(args.lhi, line)] * R.dxpow_hi[i] : 0.0;
 }
 
 // Step 1 of a build: gather the right-hand side rows of the tile (spline_builder.hpp:952-1052).
@@ -236,115 +407,6 @@ __device__ __forceinline__ void gather_tile(BuildArgs const& args, double* T)
     }
     cp_async_wait_all();
     __syncthreads();
-}
-
-// Steps 2-4 of a solve on a tile already in shared memory (T[j*TL + l] = right-hand side row j of
-// line l): forward and backward sweeps, border correction. A thread owns one chunk of a pair of
-// lines (16-byte shared-memory accesses; each factor load serves both lines). On return (after a
-// barrier) T holds the solution. Every thread of the block must call it; TL is even and the block
-// has at least nchunk * TL / 2 threads.
-template <int TL, int KL, int KU>
-__device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/, double* smem)
-{
-    static_assert(TL % 2 == 0, "the solve works on line pairs");
-    constexpr int P = TL / 2;
-    constexpr int KC = KL > KU ? KL : KU;
-    int const n = t.n, m = t.m, k = t.k;
-    int const NC = t.nchunk;
-    int const tid = threadIdx.x;
-    int const p = tid % P;
-    int const c = tid / P;
-    int const nthr = blockDim.x / P;                         // threads per pair
-    double2* const T2 = reinterpret_cast<double2*>(smem) + p;  // n rows, stride P
-    double2* const carry = T2 + (size_t)n * P;                // NC x KC rows
-    double2* const halo = carry + (size_t)NC * KC * P;       // NC x KL rows
-    double2* const btmp = halo + (size_t)NC * KL * P;        // k rows
-    double2 const zero = make_double2(0.0, 0.0);
-
-    int a = 0, e = 0;
-    if (c < NC) {
-        a = c * t.chunk_len;
-        e = (c == NC - 1) ? m : a + t.chunk_len;
-    }
-
-    // ---- 2. forward sweep with L (and the row interchanges) ----
-    if (m > 0) {
-        if (c < NC) {
-            double2 w[KL + 1];
-#pragma unroll
-            for (int q = 0; q < KL; ++q) w[q] = (a + q < m) ? T2[(a + q) * P] : zero;
-            if (t.pivot) fwd_sweep<KL, true, false>(t, T2, P, a, e, w, nullptr, 0);
-            else fwd_sweep<KL, false, false>(t, T2, P, a, e, w, nullptr, 0);
-#pragma unroll
-            for (int q = 0; q < KL; ++q) {
-                double2 const orig = (e + q < m) ? T2[(e + q) * P] : zero;
-                carry[(c * KC + q) * P] = make_double2(w[q].x - orig.x, w[q].y - orig.y);
-                if (t.pivot) halo[(c * KL + q) * P] = orig;
-            }
-        }
-        __syncthreads();
-        carry_scan<KL, KC, true>(t.PhiF, carry, P, t.nscan, NC, c);
-        if (c < NC) {
-            double2 w[KL + 1];
-#pragma unroll
-            for (int q = 0; q < KL; ++q) {
-                double2 v = (a + q < m) ? T2[(a + q) * P] : zero;
-                if (c > 0 && a + q < m) {
-                    double2 const cin = carry[((c - 1) * KC + q) * P];
-                    v.x += cin.x;
-                    v.y += cin.y;
-                }
-                w[q] = v;
-            }
-            if (t.pivot) fwd_sweep<KL, true, true>(t, T2, P, a, e, w, halo + (size_t)c * KL * P, P);
-            else fwd_sweep<KL, false, true>(t, T2, P, a, e, w, nullptr, 0);
-        }
-        __syncthreads();
-
-        // ---- 3. backward sweep with U ----
-        if (c < NC) {
-            double2 z[KU];
-#pragma unroll
-            for (int q = 0; q < KU; ++q) z[q] = zero;
-            bwd_sweep<KU, false>(t, T2, P, a, e, z);
-#pragma unroll
-            for (int q = 0; q < KU; ++q) carry[(c * KC + q) * P] = z[q];
-        }
-        __syncthreads();
-        carry_scan<KU, KC, false>(t.PhiB, carry, P, t.nscan, NC, c);
-        if (c < NC) {
-            double2 z[KU];
-#pragma unroll
-            for (int q = 0; q < KU; ++q) z[q] = (c + 1 < NC) ? carry[((c + 1) * KC + q) * P] : zero;
-            bwd_sweep<KU, true>(t, T2, P, a, e, z);
-        }
-        __syncthreads();
-    }
-
-    // ---- 4. border: x2 = S^-1 (b2 - lambda x'), x1 = x' - (Q^-1 gamma) x2 ----
-    if (k > 0) {
-        for (int r = c; r < k; r += nthr) {
-            double2 s = T2[(m + r) * P];
-            int const q1 = __ldg(t.lam_row + r + 1);
-            for (int q = __ldg(t.lam_row + r); q < q1; ++q) s = fma2(-__ldg(t.lam_val + q), T2[__ldg(t.lam_col + q) * P], s);
-            btmp[r * P] = s;
-        }
-        __syncthreads();
-        for (int r = c; r < k; r += nthr) {
-            double2 s = zero;
-            for (int q = 0; q < k; ++q) s = fma2(__ldg(t.Sinv + r * k + q), btmp[q * P], s);
-            T2[(m + r) * P] = s;
-        }
-        __syncthreads();
-        int const nq = t.qg_lo + t.qg_hi;
-        for (int q = c; q < nq; q += nthr) {
-            int const i = q < t.qg_lo ? q : m - t.qg_hi + (q - t.qg_lo);
-            double2 s = T2[i * P];
-            for (int r = 0; r < k; ++r) s = fma2(-__ldg(t.Qg + (size_t)q * k + r), T2[(m + r) * P], s);
-            T2[i * P] = s;
-        }
-        __syncthreads();
-    }
 }
 
 // Steps 1-4 of a build. On return (after a barrier) T[j*TL + l] holds solution column j of line l,

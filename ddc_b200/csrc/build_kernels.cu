@@ -82,6 +82,7 @@ int pick_nct(SolveTables const& t, int TL)
 
 bool launch_build_eval_fused(BuildArgs const& args, Evaluator const& e, int order, double* out, Lines const& lo,
                              double const* coords, Lines const& lx, cudaStream_t s);
+void launch_refine(BuildArgs const& args, int TL, int rounds, cudaStream_t s);
 
 namespace {
 BuildArgs make_build_args(Builder const& b, double* coefs, Lines const& lc, double const* vals, Lines const& lv,
@@ -146,7 +147,8 @@ void launch_build(Builder const& b, double* coefs, Lines const& lc, double const
     args.pair16 = line_pairs_aligned(vals, lv);
     args.pair16_out = line_pairs_aligned(coefs, lc);
     if (args.nlines == 0) return;
-    dispatch(args, b.tile_lines, s);
+    if (b.precision == DDCB_FP32_REFINE) launch_refine(args, b.tile_lines, b.refine_rounds, s);
+    else dispatch(args, b.tile_lines, s);
 }
 
 void launch_solve_multirhs(Builder const& b, double* rhs, long ld, long nrhs, bool transpose, cudaStream_t s)

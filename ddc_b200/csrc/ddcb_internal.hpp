@@ -74,6 +74,15 @@ struct SolveTables
     const double* Sinv;  // k x k inverse of the Schur complement S0 - l Q^-1 g
     int qg_lo, qg_hi;    // rows [0, qg_lo) and [m - qg_hi, m) of Q^-1 g are kept (rest < 1e-19)
     const double* Qg;    // (qg_lo + qg_hi) x k
+    // FP32 copies of the factor tables (the FP32 solves of the refinement mode)
+    struct F32
+    {
+        const float *Lf, *Uf, *PhiF, *PhiB, *lam_val, *Sinv, *Qg;
+    } f32;
+    // the system matrix itself in the kernel's row / column order, CSR (FP64 residuals)
+    const int* a_row;    // n+1
+    const int* a_col;
+    const double* a_val;
 };
 
 // How the right-hand side rows are gathered from the inputs and how the coefficients are placed.
@@ -129,7 +138,6 @@ struct Builder
     std::vector<int> ipiv;
     SolveTables tables {};         // device pointers
     SolveTables tables_t {};       // tables of A^T (adjoint)
-    float* tables_f32 = nullptr;   // FP32 copies (refinement mode)
     void* d_block = nullptr;       // one allocation holding every device table
     size_t d_block_bytes = 0;
     RhsMap rhs {};

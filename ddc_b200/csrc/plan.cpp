@@ -351,8 +351,11 @@ struct HostSolve
     // rows: the system in kernel order (the builder rotates the reference's boundary rows and
     // columns to the end); border: the number of trailing rows/cols solved through the Schur
     // complement (periodic systems: derived from the circular bandwidth instead).
+    SparseRows sys; // the system in kernel order (kept for the FP64 residuals of the refinement)
+
     void analyse(SparseRows const& rows, bool periodic, long border)
     {
+        sys = rows;
         n = long(rows.size());
         k = border;
         if (periodic) {
@@ -758,6 +761,31 @@ SolveTables upload_tables(HostSolve const& h, std::vector<char>& blob, std::vect
     push(h.lam_val.data(), h.lam_val.size() * 8);
     push(h.Sinv.data(), h.Sinv.size() * 8);
     push(h.qg_rows.data(), h.qg_rows.size() * 8);
+    // FP32 copies of the factor tables, in the order of SolveTables::F32
+    auto push32 = [&](std::vector<double> const& v) {
+        std::vector<float> f(v.begin(), v.end());
+        push(f.data(), f.size() * 4);
+    };
+    push32(Lc);
+    push32(Uc);
+    push32(h.PhiF);
+    push32(h.PhiB);
+    push32(h.lam_val);
+    push32(h.Sinv);
+    push32(h.qg_rows);
+    // the system matrix, CSR in kernel order
+    std::vector<int> arow(1, 0), acol;
+    std::vector<double> aval;
+    for (auto const& r : h.sys) {
+        for (auto const& [j, v] : r) {
+            acol.push_back(int(j));
+            aval.push_back(v);
+        }
+        arow.push_back(int(acol.size()));
+    }
+    push(arow.data(), arow.size() * 4);
+    push(acol.data(), acol.size() * 4);
+    push(aval.data(), aval.size() * 8);
     return t;
 }
 
@@ -773,6 +801,16 @@ void bind_tables(SolveTables& t, char* base, size_t const* offs)
     t.lam_val = reinterpret_cast<double const*>(base + offs[7]);
     t.Sinv = reinterpret_cast<double const*>(base + offs[8]);
     t.Qg = reinterpret_cast<double const*>(base + offs[9]);
+    t.f32.Lf = reinterpret_cast<float const*>(base + offs[10]);
+    t.f32.Uf = reinterpret_cast<float const*>(base + offs[11]);
+    t.f32.PhiF = reinterpret_cast<float const*>(base + offs[12]);
+    t.f32.PhiB = reinterpret_cast<float const*>(base + offs[13]);
+    t.f32.lam_val = reinterpret_cast<float const*>(base + offs[14]);
+    t.f32.Sinv = reinterpret_cast<float const*>(base + offs[15]);
+    t.f32.Qg = reinterpret_cast<float const*>(base + offs[16]);
+    t.a_row = reinterpret_cast<int const*>(base + offs[17]);
+    t.a_col = reinterpret_cast<int const*>(base + offs[18]);
+    t.a_val = reinterpret_cast<double const*>(base + offs[19]);
 }
 
 std::string describe(HostSolve const& h)
