@@ -59,6 +59,13 @@ class BuilderInfo(C.Structure):
                 ("pivoting", C.c_int32), ("chunks", C.c_int32), ("tile_lines", C.c_int32)]
 
 
+class UnevenInfo(C.Structure):
+    _fields_ = [("count", C.c_int64), ("total_vals", C.c_int64), ("total_derivs_lo", C.c_int64),
+                ("total_derivs_hi", C.c_int64), ("total_coefs", C.c_int64), ("total_evals", C.c_int64),
+                ("threads", C.c_int32), ("blocks_per_sm", C.c_int32), ("order", C.c_int32),
+                ("shared_bytes", C.c_int32), ("tuned_us", C.c_double)]
+
+
 _vp = C.c_void_p
 _dp = C.POINTER(C.c_double)
 _pp = C.POINTER(C.c_void_p)
@@ -83,6 +90,12 @@ SIGNATURES = {
     "ddcb_eval": [_vp, _vp, Lines, _vp, Lines, _vp, Lines, _vp],
     "ddcb_eval_deriv": [_vp, C.c_int32, _vp, Lines, _vp, Lines, _vp, Lines, _vp],
     "ddcb_integrate": [_vp, _vp, C.c_int64, _vp, Lines, _vp],
+    "ddcb_batch_uneven_create": [_vp, _vp, _vp, C.c_int64, _pp],
+    "ddcb_batch_uneven_destroy": [_vp],
+    "ddcb_batch_uneven_get_info": [_vp, C.POINTER(UnevenInfo)],
+    "ddcb_batch_uneven_offsets": [_vp, _vp, _vp, _vp, _vp, _vp],
+    "ddcb_batch_uneven_tune": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int32, _vp],
+    "ddcb_batch_uneven_run": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "ddcb_build2d_workspace_bytes": [_vp, _vp, C.c_int64, C.POINTER(C.c_uint64)],
     "ddcb_build2d": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int64, _vp, C.c_uint64, _vp],
     "ddcb_eval2d": [_vp, _vp, C.c_int32, C.c_int32, _vp, _vp, _vp, C.c_int64, C.c_int64, _vp],

@@ -531,8 +531,9 @@ void launch_build_adjoint(Builder const& b, double const* gc, Lines const& lgc, 
 {
     AdjointArgs a = make_adjoint_args(b, gc, lgc, gv, lgv, gdlo, lglo, gdhi, lghi);
     if (a.nlines == 0) return;
-    a.nct = adj_nct(a.t, b.tile_lines, 128);
-    dispatch_build_adjoint(a, b.tile_lines, s);
+    int const TL = fit_tile_lines(b.tile_lines, [&](int w) { return sizeof(double) * tile_doubles(a.t, w, a.t.kl, a.t.ku); });
+    a.nct = adj_nct(a.t, TL, 128);
+    dispatch_build_adjoint(a, TL, s);
 }
 
 void launch_eval_adjoint(Evaluator const& e, int order, double const* coords, Lines const& lx, double const* coefs,

@@ -585,6 +585,110 @@ ddcb_status ddcb_build_eval_adjoint(ddcb_builder h, ddcb_evaluator he, int32_t o
     });
 }
 
+struct ddcb_uneven_batch_t
+{
+    ddcb::UnevenBatch* b = nullptr;
+};
+
+ddcb_status ddcb_batch_uneven_create(const ddcb_builder* builders, const ddcb_evaluator* evaluators, const int64_t* nevals,
+                                     int64_t count, ddcb_uneven_batch* out)
+{
+    return guarded([&] {
+        require(out != nullptr, "out is NULL");
+        *out = nullptr;
+        require(count >= 0 && count < (int64_t(1) << 30), "bad problem count");
+        require(count == 0 || (builders && evaluators && nevals), "NULL problem arrays");
+        std::vector<ddcb::Builder const*> bl(static_cast<size_t>(count));
+        std::vector<ddcb::Evaluator const*> ev(static_cast<size_t>(count));
+        for (int64_t i = 0; i < count; ++i) {
+            require(builders[i] != nullptr && evaluators[i] != nullptr, "NULL builder or evaluator in the batch");
+            bl[size_t(i)] = builders[i]->b;
+            ev[size_t(i)] = evaluators[i]->e;
+        }
+        auto* h = new ddcb_uneven_batch_t();
+        try {
+            h->b = ddcb::create_uneven_batch(bl.data(), ev.data(), nevals, count);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+ddcb_status ddcb_batch_uneven_destroy(ddcb_uneven_batch h)
+{
+    return guarded([&] {
+        if (!h) return;
+        ddcb::destroy_uneven_batch(h->b);
+        delete h;
+    });
+}
+
+ddcb_status ddcb_batch_uneven_get_info(ddcb_uneven_batch h, ddcb_uneven_info* info)
+{
+    return guarded([&] {
+        require(h != nullptr && info != nullptr, "NULL argument");
+        int64_t tot[6];
+        int sch[4];
+        double us = 0.0;
+        ddcb::uneven_info(*h->b, tot, sch, &us);
+        info->count = tot[0];
+        info->total_vals = tot[1];
+        info->total_derivs_lo = tot[2];
+        info->total_derivs_hi = tot[3];
+        info->total_coefs = tot[4];
+        info->total_evals = tot[5];
+        info->threads = sch[0];
+        info->blocks_per_sm = sch[1];
+        info->order = sch[2];
+        info->shared_bytes = sch[3];
+        info->tuned_us = us;
+    });
+}
+
+ddcb_status ddcb_batch_uneven_offsets(ddcb_uneven_batch h, int64_t* vals, int64_t* dlo, int64_t* dhi, int64_t* coefs,
+                                      int64_t* evals)
+{
+    return guarded([&] {
+        require(h != nullptr, "batch is NULL");
+        ddcb::uneven_offsets(*h->b, vals, dlo, dhi, coefs, evals);
+    });
+}
+
+static void check_uneven_buffers(ddcb_uneven_batch h, const double* vals, const double* dlo, const double* dhi,
+                                 double* coefs, const double* coords, double* out)
+{
+    require(h != nullptr, "batch is NULL");
+    int64_t tot[6];
+    int sch[4];
+    double us;
+    ddcb::uneven_info(*h->b, tot, sch, &us);
+    require(tot[1] == 0 || vals, "vals is NULL");
+    require(tot[2] == 0 || dlo, "derivs_lo is NULL");
+    require(tot[3] == 0 || dhi, "derivs_hi is NULL");
+    require(tot[4] == 0 || coefs, "coefs is NULL");
+    require(tot[5] == 0 || (coords && out), "coords/out is NULL");
+}
+
+ddcb_status ddcb_batch_uneven_tune(ddcb_uneven_batch h, const double* vals, const double* dlo, const double* dhi,
+                                   double* coefs, const double* coords, double* out, int32_t reps, ddcb_stream stream)
+{
+    return guarded([&] {
+        check_uneven_buffers(h, vals, dlo, dhi, coefs, coords, out);
+        ddcb::tune_uneven_batch(*h->b, vals, dlo, dhi, coefs, coords, out, reps, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+ddcb_status ddcb_batch_uneven_run(ddcb_uneven_batch h, const double* vals, const double* dlo, const double* dhi,
+                                  double* coefs, const double* coords, double* out, ddcb_stream stream)
+{
+    return guarded([&] {
+        check_uneven_buffers(h, vals, dlo, dhi, coefs, coords, out);
+        ddcb::run_uneven_batch(*h->b, vals, dlo, dhi, coefs, coords, out, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
 ddcb_status ddcb_build2d_workspace_bytes(ddcb_builder b1, ddcb_builder b2, int64_t nbatch, uint64_t* bytes)
 {
     return guarded([&] {

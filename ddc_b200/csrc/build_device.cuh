@@ -37,7 +37,15 @@ struct BuildArgs
     int nct;            // chunk threads per line (block = TL * nct)
     int pair16;         // vals: adjacent line pairs are 16-byte aligned and contiguous
     int pair16_out;     // out: the same for the coefficient output
+    int64_t line_base;  // first line of the block's tile; < 0: blockIdx.x * TL
 };
+
+// First line of the block's tile.
+template <int TL>
+__device__ __forceinline__ int64_t tile_line0(BuildArgs const& args)
+{
+    return args.line_base >= 0 ? args.line_base : (int64_t)blockIdx.x * TL;
+}
 
 
 __device__ __forceinline__ int64_t line_offset(Lines const& L, int64_t b)
@@ -115,14 +123,14 @@ struct Fac<float>
 // (WRITE false) reads rows beyond e from the tile, which nothing has written yet. Phase C (WRITE
 // true) writes rows a..e-1; without interchanges rows beyond e only feed the next chunk's rows,
 // so they are not read; with interchanges they come from the halo copy.
-template <class R, int KL, bool PIV, bool WRITE>
+template <class R, int KL, bool PIV, bool WRITE, int UNR>
 __device__ __forceinline__ void fwd_sweep(SolveTables const& t, typename Fac<R>::V* T2, int P, int a, int e,
                                           typename Fac<R>::V* w, const typename Fac<R>::V* halo, int hstride)
 {
     using V = typename Fac<R>::V;
     R const* __restrict__ Lf = Fac<R>::Lf(t);
     int const lim = (WRITE && !PIV) ? e : t.m; // fill rows below lim are read
-#pragma unroll 4
+#pragma unroll UNR
     for (int j = a; j < e; ++j) {
         int const rr = j + KL;
         V fill = Fac<R>::zero();
@@ -152,13 +160,13 @@ __device__ __forceinline__ void fwd_sweep(SolveTables const& t, typename Fac<R>:
 
 // Backward sweep with U over rows e-1 .. a of a line pair; z[0..KU-1] hold the solution rows
 // e .. e+KU-1 (the carry from the chunk below) on entry.
-template <class R, int KU, bool WRITE>
+template <class R, int KU, bool WRITE, int UNR>
 __device__ __forceinline__ void bwd_sweep(SolveTables const& t, typename Fac<R>::V* T2, int P, int a, int e,
                                           typename Fac<R>::V* z)
 {
     using V = typename Fac<R>::V;
     R const* __restrict__ Uf = Fac<R>::Uf(t);
-#pragma unroll 4
+#pragma unroll UNR
     for (int j = e - 1; j >= a; --j) {
         R const* U = Uf + (size_t)crow(t, j) * (KU + 1);
         V s = T2[j * P];
@@ -221,6 +229,19 @@ __host__ __device__ inline size_t tile_doubles(SolveTables const& t, int TL, int
     return (size_t)t.n * TL + (size_t)t.nchunk * KC * TL + (size_t)t.nchunk * KL * TL + (size_t)t.k * TL;
 }
 
+// Largest tile width in {TL, TL/2, ..., 2} whose shared memory (bytes(width)) fits in the
+// device's per-block opt-in limit; TL itself when none does (the launch then reports it).
+template <class Bytes>
+inline int fit_tile_lines(int TL, Bytes bytes)
+{
+    int dev = 0, optin = 0;
+    DDCB_CUDA_CHECK(cudaGetDevice(&dev));
+    DDCB_CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    for (int w = TL; w >= 2; w /= 2)
+        if (bytes(w) <= size_t(optin)) return w;
+    return TL;
+}
+
 // Steps 2-4 of a solve on a tile already in shared memory (T[j*TL + l] = right-hand side row j of
 // line l, in the arithmetic type R): forward and backward sweeps, border correction. A thread owns
 // one chunk of a pair of lines (paired shared-memory accesses; each factor load serves both
@@ -234,6 +255,8 @@ __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/,
     using V = typename Fac<R>::V;
     constexpr int P = TL / 2;
     constexpr int KC = KL > KU ? KL : KU;
+    constexpr int UNR = TL >= 4 ? 4 : 1; // rows unrolled per sweep step; a single line pair is not
+                                         // unrolled, which keeps its kernels free of spills
     int const n = t.n, m = t.m, k = t.k;
     int const NC = t.nchunk;
     int const tid = threadIdx.x;
@@ -258,8 +281,8 @@ __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/,
             V w[KL + 1];
 #pragma unroll
             for (int q = 0; q < KL; ++q) w[q] = (a + q < m) ? T2[(a + q) * P] : zero;
-            if (t.pivot) fwd_sweep<R, KL, true, false>(t, T2, P, a, e, w, nullptr, 0);
-            else fwd_sweep<R, KL, false, false>(t, T2, P, a, e, w, nullptr, 0);
+            if (t.pivot) fwd_sweep<R, KL, true, false, UNR>(t, T2, P, a, e, w, nullptr, 0);
+            else fwd_sweep<R, KL, false, false, UNR>(t, T2, P, a, e, w, nullptr, 0);
 #pragma unroll
             for (int q = 0; q < KL; ++q) {
                 V const orig = (e + q < m) ? T2[(e + q) * P] : zero;
@@ -277,8 +300,8 @@ __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/,
                 if (c > 0 && a + q < m) v = add2(v, carry[((c - 1) * KC + q) * P]);
                 w[q] = v;
             }
-            if (t.pivot) fwd_sweep<R, KL, true, true>(t, T2, P, a, e, w, halo + (size_t)c * KL * P, P);
-            else fwd_sweep<R, KL, false, true>(t, T2, P, a, e, w, nullptr, 0);
+            if (t.pivot) fwd_sweep<R, KL, true, true, UNR>(t, T2, P, a, e, w, halo + (size_t)c * KL * P, P);
+            else fwd_sweep<R, KL, false, true, UNR>(t, T2, P, a, e, w, nullptr, 0);
         }
         __syncthreads();
 
@@ -287,7 +310,7 @@ __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/,
             V z[KU];
 #pragma unroll
             for (int q = 0; q < KU; ++q) z[q] = zero;
-            bwd_sweep<R, KU, false>(t, T2, P, a, e, z);
+            bwd_sweep<R, KU, false, UNR>(t, T2, P, a, e, z);
 #pragma unroll
             for (int q = 0; q < KU; ++q) carry[(c * KC + q) * P] = z[q];
         }
@@ -297,7 +320,7 @@ __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/,
             V z[KU];
 #pragma unroll
             for (int q = 0; q < KU; ++q) z[q] = (c + 1 < NC) ? carry[((c + 1) * KC + q) * P] : zero;
-            bwd_sweep<R, KU, true>(t, T2, P, a, e, z);
+            bwd_sweep<R, KU, true, UNR>(t, T2, P, a, e, z);
         }
         __syncthreads();
     }
@@ -373,7 +396,7 @@ __device__ __forceinline__ void gather_tile(BuildArgs const& args, double* T)
         // solve tables resident there
         int const p = tid % (TL / 2);
         int const c2 = tid / (TL / 2);
-        int64_t const line = (int64_t)blockIdx.x * TL + 2 * p;
+        int64_t const line = tile_line0<TL>(args) + 2 * p;
         bool const live0 = line < args.nlines, live1 = line + 1 < args.nlines;
         int64_t const ov = live0 ? line_offset(args.lv, line) : 0;
         for (int r = c2; r < n; r += 2 * nct) {
@@ -395,7 +418,7 @@ __device__ __forceinline__ void gather_tile(BuildArgs const& args, double* T)
     } else {
         int const l = tid % TL;
         int const c = tid / TL;
-        int64_t const line = (int64_t)blockIdx.x * TL + l;
+        int64_t const line = tile_line0<TL>(args) + l;
         bool const live = line < args.nlines;
         int64_t const ov = live ? line_offset(args.lv, line) : 0;
         for (int r = c; r < n; r += nct) {
@@ -440,7 +463,7 @@ __device__ __forceinline__ void store_tile(BuildArgs const& args, const double* 
     if (TL % 2 == 0 && args.pair16_out) {
         int const p = tid % (TL / 2);
         int const c2 = tid / (TL / 2);
-        int64_t const line = (int64_t)blockIdx.x * TL + 2 * p;
+        int64_t const line = tile_line0<TL>(args) + 2 * p;
         if (line >= args.nlines) return;
         int64_t const oo = line_offset(args.lo, line);
         bool const live1 = line + 1 < args.nlines;
@@ -454,7 +477,7 @@ __device__ __forceinline__ void store_tile(BuildArgs const& args, const double* 
     }
     int const l = tid % TL;
     int const c = tid / TL;
-    int64_t const line = (int64_t)blockIdx.x * TL + l;
+    int64_t const line = tile_line0<TL>(args) + l;
     if (line >= args.nlines) return;
     int64_t const oo = line_offset(args.lo, line);
     for (int r = c; r < rows; r += args.nct) __stcs(args.out + r * args.lo.stride + oo, T[coef_row(args.r, n, r) * TL + l]);

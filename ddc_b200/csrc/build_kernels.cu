@@ -89,6 +89,7 @@ BuildArgs make_build_args(Builder const& b, double* coefs, Lines const& lc, doub
                           double const* dlo, Lines const& llo, double const* dhi, Lines const& lhi)
 {
     BuildArgs args {};
+    args.line_base = -1;
     args.t = b.tables;
     args.r = b.rhs;
     args.raw = 0;
@@ -131,6 +132,7 @@ void launch_build(Builder const& b, double* coefs, Lines const& lc, double const
                   double const* dlo, Lines const& llo, double const* dhi, Lines const& lhi, cudaStream_t s)
 {
     BuildArgs args {};
+    args.line_base = -1;
     args.t = b.tables;
     args.r = b.rhs;
     args.raw = 0;
@@ -147,13 +149,24 @@ void launch_build(Builder const& b, double* coefs, Lines const& lc, double const
     args.pair16 = line_pairs_aligned(vals, lv);
     args.pair16_out = line_pairs_aligned(coefs, lc);
     if (args.nlines == 0) return;
-    if (b.precision == DDCB_FP32_REFINE) launch_refine(args, b.tile_lines, b.refine_rounds, s);
-    else dispatch(args, b.tile_lines, s);
+    // long lines: fewer lines per tile, so that the tile fits in shared memory
+    int const kl = b.tables.kl, ku = b.tables.ku;
+    int TL;
+    if (b.precision == DDCB_FP32_REFINE)
+        TL = fit_tile_lines(b.tile_lines, [&](int w) {
+            return sizeof(double) * (size_t)b.tables.n * w + sizeof(float) * tile_doubles(b.tables, w, kl, ku) + 16;
+        });
+    else
+        TL = fit_tile_lines(b.tile_lines, [&](int w) { return sizeof(double) * tile_doubles(b.tables, w, kl, ku); });
+    args.nct = pick_nct(b.tables, TL);
+    if (b.precision == DDCB_FP32_REFINE) launch_refine(args, TL, b.refine_rounds, s);
+    else dispatch(args, TL, s);
 }
 
 void launch_solve_multirhs(Builder const& b, double* rhs, long ld, long nrhs, bool transpose, cudaStream_t s)
 {
     BuildArgs args {};
+    args.line_base = -1;
     args.t = transpose ? b.tables_t : b.tables;
     args.r = b.rhs;
     args.raw = 1;
@@ -170,7 +183,9 @@ void launch_solve_multirhs(Builder const& b, double* rhs, long ld, long nrhs, bo
     args.nct = pick_nct(args.t, b.tile_lines);
     args.pair16 = args.pair16_out = line_pairs_aligned(rhs, L);
     if (nrhs == 0) return;
-    dispatch(args, b.tile_lines, s);
+    int const TL = fit_tile_lines(b.tile_lines, [&](int w) { return sizeof(double) * tile_doubles(args.t, w, args.t.kl, args.t.ku); });
+    args.nct = pick_nct(args.t, TL);
+    dispatch(args, TL, s);
 }
 
 } // namespace ddcb

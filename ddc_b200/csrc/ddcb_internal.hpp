@@ -197,6 +197,18 @@ bool launch_build_eval_adjoint(Builder const& b, Evaluator const& e, int order, 
                                Lines const& lgv, double* gdlo, Lines const& lglo, double* gdhi, Lines const& lghi,
                                double* gx, Lines const& lgx, cudaStream_t s);
 
+// uneven_batch.cu
+struct UnevenBatch;
+UnevenBatch* create_uneven_batch(Builder const* const* builders, Evaluator const* const* evals, int64_t const* nevals,
+                                 int64_t count);
+void destroy_uneven_batch(UnevenBatch* b);
+void uneven_offsets(UnevenBatch const& b, int64_t* vals, int64_t* dlo, int64_t* dhi, int64_t* coefs, int64_t* evals);
+void uneven_info(UnevenBatch const& b, int64_t* totals, int* schedule, double* tuned_us);
+void run_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, double const* dhi, double* coefs,
+                      double const* coords, double* out, cudaStream_t s);
+void tune_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, double const* dhi, double* coefs,
+                       double const* coords, double* out, int reps, cudaStream_t s);
+
 // tensor2d.cu
 size_t build2d_workspace_bytes(Builder const& b1, Builder const& b2, int64_t nbatch);
 void launch_build2d(Builder const& b1, Builder const& b2, double* coefs, double const* vals, double const* dmin1,

@@ -174,9 +174,14 @@ void launch_eval(Evaluator const& e, int order, double* out, Lines const& lo, do
     a.lo = lo;
     a.pair16 = line_pairs_aligned(coefs, lc);
     if (a.nlines == 0 || lx.n == 0) return;
-    constexpr int TLE = 8;
-    size_t sm = sizeof(double) * ((size_t)a.size * TLE + (e.eb.b.uniform ? 0 : 2 * (size_t)e.eb.nk));
-    launch_deg<TLE>(a, order, sm, s);
+    // eight lines per block; two when the coefficient tile of eight long lines does not fit
+    auto bytes = [&](int tle) { return sizeof(double) * ((size_t)a.size * tle + (e.eb.b.uniform ? 0 : 2 * (size_t)e.eb.nk)); };
+    int dev = 0, optin = 0;
+    DDCB_CUDA_CHECK(cudaGetDevice(&dev));
+    DDCB_CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (bytes(8) <= size_t(optin)) launch_deg<8>(a, order, bytes(8), s);
+    else if (bytes(2) <= size_t(optin)) launch_deg<2>(a, order, bytes(2), s);
+    else throw Error(DDCB_ERR_UNSUPPORTED, "a line of " + std::to_string(a.size) + " coefficients exceeds the evaluator's shared-memory tile");
 }
 
 void launch_integrate(Evaluator const& e, double* out, int64_t out_outer_stride, double const* coefs, Lines const& lc,

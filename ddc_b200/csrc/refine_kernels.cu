@@ -27,7 +27,7 @@ __device__ __forceinline__ void residual_tile(BuildArgs const& args, const doubl
     int const l = threadIdx.x % TL;
     int const c = threadIdx.x / TL;
     int const nct = blockDim.x / TL;
-    int64_t const line = (int64_t)blockIdx.x * TL + l;
+    int64_t const line = tile_line0<TL>(args) + l;
     bool const live = line < args.nlines;
     for (int r = c; r < n; r += nct) {
         double s = live ? rhs_row(args, r, line) : 0.0;

@@ -1,0 +1,465 @@
+// uneven_batch.cu -- thousands of independent 1D spline problems of different size, degree,
+// closure and mesh, built and evaluated by persistent kernels in ONE graph launch.
+//
+// Each problem is one line: a builder (its device factor tables) and an evaluator, with its
+// samples, derivatives, coefficients, coordinates and values packed one after another in flat
+// arrays. Problems are grouped by the band shape of their factors (the solve is compiled per
+// shape: one kernel holding every shape's solve spills registers). Each group gets a persistent
+// kernel with a fixed grid (its share of blocks_per_sm x SMs, in proportion to its work); every
+// block takes the group's next problem from a counter (largest-first order by default, so the long
+// problems start early and the short ones fill the tail), builds it in shared memory with the same
+// chunked tile solve as the batched builder (a line pair whose second line is empty), stores its
+// coefficients and evaluates its points from the solved tile. The per-problem description is
+// copied into shared memory once per problem, so the solve reads its tables' addresses from there.
+//
+// ddcb_batch_uneven_run launches a CUDA graph holding the counter reset and the group kernels,
+// which run concurrently; the graph is rebuilt only when the buffers, stream or schedule change.
+// ddcb_batch_uneven_tune times the candidate schedules (block size, blocks per SM, queue order),
+// each as the graph it would run as, on the caller's buffers and keeps the fastest.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+#include "build_device.cuh"
+#include "eval_device.cuh"
+
+namespace ddcb {
+
+// Band shapes of the plan's menu (plan.cpp, HostSolve::analyse), by index.
+static int const kShapes[][2] = {{1, 1}, {1, 2}, {2, 2}, {3, 3}, {1, 4}, {2, 4}, {4, 4}, {3, 6}, {1, 8}, {2, 8}, {4, 8}};
+static int const kNumShapes = int(sizeof(kShapes) / sizeof(kShapes[0]));
+
+struct UnevenProblem
+{
+    BuildArgs args;        // data pointers hold offsets into the packed arrays (added at run time)
+    EvalBasis eb;
+    int ex_lo, ex_hi;
+    int shape;             // index into kShapes
+    int degree, uniform;
+    int m;                 // evaluation points
+    int64_t x_off, out_off;
+};
+
+struct UnevenArgs
+{
+    const UnevenProblem* probs;
+    const int* order;      // queue order of the group's problems
+    int nprob;
+    int* counter;          // next queue position (reset to 0 before each launch)
+    const double* vals;
+    const double* dlo;
+    const double* dhi;
+    double* coefs;
+    const double* coords;
+    double* out;
+};
+
+namespace {
+
+template <int D, bool UNI>
+__device__ __noinline__ void eval_line(EvalBasis const& eb, int ex_lo, int ex_hi, CoefRotated const& acc,
+                                       const double* __restrict__ x, double* __restrict__ out, int m)
+{
+    for (int q = threadIdx.x; q < m; q += blockDim.x) __stcs(out + q, eval_point<D, 0, UNI>(eb, ex_lo, ex_hi, __ldcs(x + q), acc));
+}
+
+__device__ __forceinline__ void eval_any(int degree, int uniform, EvalBasis const& eb, int ex_lo, int ex_hi,
+                                         CoefRotated const& acc, const double* x, double* out, int m)
+{
+    switch (degree * 2 + uniform) {
+    case 2: eval_line<1, false>(eb, ex_lo, ex_hi, acc, x, out, m); break;
+    case 3: eval_line<1, true>(eb, ex_lo, ex_hi, acc, x, out, m); break;
+    case 4: eval_line<2, false>(eb, ex_lo, ex_hi, acc, x, out, m); break;
+    case 5: eval_line<2, true>(eb, ex_lo, ex_hi, acc, x, out, m); break;
+    case 6: eval_line<3, false>(eb, ex_lo, ex_hi, acc, x, out, m); break;
+    case 7: eval_line<3, true>(eb, ex_lo, ex_hi, acc, x, out, m); break;
+    case 8: eval_line<4, false>(eb, ex_lo, ex_hi, acc, x, out, m); break;
+    case 9: eval_line<4, true>(eb, ex_lo, ex_hi, acc, x, out, m); break;
+    case 10: eval_line<5, false>(eb, ex_lo, ex_hi, acc, x, out, m); break;
+    default: eval_line<5, true>(eb, ex_lo, ex_hi, acc, x, out, m); break;
+    }
+}
+
+template <int KL, int KU>
+__global__ void __launch_bounds__(512) uneven_kernel(const __grid_constant__ UnevenArgs A)
+{
+    extern __shared__ __align__(16) double smem[];
+    __shared__ UnevenProblem sp;
+    __shared__ int s_next;
+    for (;;) {
+        if (threadIdx.x == 0) s_next = atomicAdd(A.counter, 1);
+        __syncthreads();
+        int const qi = s_next;
+        if (qi >= A.nprob) break;
+        // the problem's description into shared memory, offsets turned into pointers
+        {
+            const int* src = reinterpret_cast<const int*>(A.probs + A.order[qi]);
+            int* dst = reinterpret_cast<int*>(&sp);
+            for (int i = threadIdx.x; i < int(sizeof(UnevenProblem) / sizeof(int)); i += blockDim.x) dst[i] = __ldg(src + i);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            sp.args.vals = A.vals + reinterpret_cast<intptr_t>(sp.args.vals);
+            sp.args.dlo = A.dlo + reinterpret_cast<intptr_t>(sp.args.dlo);
+            sp.args.dhi = A.dhi + reinterpret_cast<intptr_t>(sp.args.dhi);
+            sp.args.out = A.coefs + reinterpret_cast<intptr_t>(sp.args.out);
+            sp.args.nct = blockDim.x / 2;
+        }
+        __syncthreads();
+        gather_tile<2>(sp.args, smem);
+        solve_in_tile<2, KL, KU>(sp.args.t, 0, smem);
+        store_tile<2>(sp.args, smem);
+        CoefRotated const acc {smem, 2, sp.args.t.n, sp.args.r.srot};
+        eval_any(sp.degree, sp.uniform, sp.eb, sp.ex_lo, sp.ex_hi, acc, A.coords + sp.x_off, A.out + sp.out_off, sp.m);
+        __syncthreads(); // the tile and the description are reused by the next problem
+    }
+}
+
+using UnevenKernel = void (*)(UnevenArgs);
+
+UnevenKernel kernel_of(int shape)
+{
+    switch (shape) {
+    case 0: return uneven_kernel<1, 1>;
+    case 1: return uneven_kernel<1, 2>;
+    case 2: return uneven_kernel<2, 2>;
+    case 3: return uneven_kernel<3, 3>;
+    case 4: return uneven_kernel<1, 4>;
+    case 5: return uneven_kernel<2, 4>;
+    case 6: return uneven_kernel<4, 4>;
+    case 7: return uneven_kernel<3, 6>;
+    case 8: return uneven_kernel<1, 8>;
+    case 9: return uneven_kernel<2, 8>;
+    default: return uneven_kernel<4, 8>;
+    }
+}
+
+size_t problem_smem(UnevenProblem const& p)
+{
+    return sizeof(double) * tile_doubles(p.args.t, 2, kShapes[p.shape][0], kShapes[p.shape][1]);
+}
+
+} // namespace
+
+struct UnevenBatch
+{
+    int device = -1;
+    int64_t count = 0;
+    std::vector<int64_t> vals_off, dlo_off, dhi_off, coef_off, x_off; // count + 1 prefix sums
+    UnevenProblem* d_probs = nullptr;
+    // per band-shape group: its problems in two queue orders (largest-first, then natural) at
+    // d_order + 2*gfirst[g] and d_order + 2*gfirst[g] + gsize[g]; its counter d_counter[g]
+    std::vector<int> gshape, gfirst, gsize;
+    std::vector<double> gcost;
+    std::vector<size_t> gsmem;
+    int* d_order = nullptr;
+    int* d_counter = nullptr;
+    size_t smem = 0;
+    int max_chunks = 0;
+    // schedule
+    int threads = 256;
+    int blocks_per_sm = 0;     // 0: as many as fit
+    int order = 0;             // 0 largest-first, 1 natural
+    double tuned_us = 0.0;
+    // cached graph
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    UnevenArgs key {};
+    cudaStream_t key_stream = nullptr;
+    int key_threads = 0, key_blocks = 0, key_order = -1;
+};
+
+namespace {
+
+int sm_count()
+{
+    int dev = 0, sms = 0;
+    DDCB_CUDA_CHECK(cudaGetDevice(&dev));
+    DDCB_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    return sms;
+}
+
+// Blocks of group g's kernel: its share (by work) of per_sm (0: as many as fit) blocks per SM
+// over the SMs, at least one, at most its problem count.
+int group_blocks(UnevenBatch const& b, int g, int threads, int per_sm)
+{
+    UnevenKernel k = kernel_of(b.gshape[size_t(g)]);
+    size_t const sm = b.gsmem[size_t(g)];
+    if (sm > 48 * 1024) DDCB_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    int fit = 0;
+    DDCB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k, threads, sm));
+    if (fit < 1) throw Error(DDCB_ERR_UNSUPPORTED, "the largest problem's tile does not fit in shared memory");
+    int const per = per_sm > 0 ? std::min(per_sm, fit) : fit;
+    double total = 0.0;
+    for (double c : b.gcost) total += c;
+    double const share = total > 0.0 ? b.gcost[size_t(g)] / total : 1.0;
+    int64_t const blocks = std::llround(share * per * sm_count());
+    return int(std::max<int64_t>(1, std::min<int64_t>(blocks, b.gsize[size_t(g)])));
+}
+
+UnevenArgs make_args(UnevenBatch const& b, int g, int order, double const* vals, double const* dlo, double const* dhi,
+                     double* coefs, double const* coords, double* out)
+{
+    UnevenArgs a {};
+    a.probs = b.d_probs;
+    a.order = b.d_order + 2 * b.gfirst[size_t(g)] + (order ? b.gsize[size_t(g)] : 0);
+    a.nprob = b.gsize[size_t(g)];
+    a.counter = b.d_counter + g;
+    a.vals = vals;
+    a.dlo = dlo;
+    a.dhi = dhi;
+    a.coefs = coefs;
+    a.coords = coords;
+    a.out = out;
+    return a;
+}
+
+void drop_graph(UnevenBatch& b)
+{
+    if (b.exec) cudaGraphExecDestroy(b.exec);
+    if (b.graph) cudaGraphDestroy(b.graph);
+    b.exec = nullptr;
+    b.graph = nullptr;
+}
+
+} // namespace
+
+UnevenBatch* create_uneven_batch(Builder const* const* builders, Evaluator const* const* evals, int64_t const* nevals,
+                                 int64_t count)
+{
+    auto* b = new UnevenBatch();
+    try {
+        DDCB_CUDA_CHECK(cudaGetDevice(&b->device));
+        b->count = count;
+        std::vector<UnevenProblem> probs(static_cast<size_t>(count));
+        b->vals_off.assign(size_t(count) + 1, 0);
+        b->dlo_off = b->dhi_off = b->coef_off = b->x_off = b->vals_off;
+        std::vector<double> cost(static_cast<size_t>(count));
+        for (int64_t i = 0; i < count; ++i) {
+            Builder const& bl = *builders[i];
+            Evaluator const& ev = *evals[i];
+            std::string const who = "problem " + std::to_string(i) + ": ";
+            if (bl.device != b->device || ev.device != b->device) throw Error(DDCB_ERR_INVALID_ARGUMENT, who + "created for another device");
+            if (bl.precision != DDCB_FP64) throw Error(DDCB_ERR_UNSUPPORTED, who + "the uneven batch runs the FP64 solve");
+            if (ev.basis.desc.degree != bl.basis.desc.degree || ev.basis.desc.ncells != bl.basis.desc.ncells
+                || ev.basis.desc.periodic != bl.basis.desc.periodic || ev.basis.desc.uniform != bl.basis.desc.uniform)
+                throw Error(DDCB_ERR_INVALID_ARGUMENT, who + "builder and evaluator use different bases");
+            if (nevals[i] < 0 || nevals[i] > (int64_t(1) << 30)) throw Error(DDCB_ERR_INVALID_ARGUMENT, who + "bad evaluation count");
+            UnevenProblem& p = probs[size_t(i)];
+            p.shape = -1;
+            for (int sh = 0; sh < kNumShapes; ++sh)
+                if (kShapes[sh][0] == bl.tables.kl && kShapes[sh][1] == bl.tables.ku) p.shape = sh;
+            if (p.shape < 0) throw Error(DDCB_ERR_UNSUPPORTED, who + "band shape has no kernel");
+            if (bl.tables.nchunk > 512) throw Error(DDCB_ERR_UNSUPPORTED, who + "more than 512 chunks per line");
+            int64_t const np = int64_t(bl.points.size()), size = int64_t(bl.basis.size());
+            b->vals_off[i + 1] = b->vals_off[i] + np;
+            b->dlo_off[i + 1] = b->dlo_off[i] + (bl.lo == DDCB_HERMITE ? bl.nbv_lo : 0);
+            b->dhi_off[i + 1] = b->dhi_off[i] + (bl.hi == DDCB_HERMITE ? bl.nbv_hi : 0);
+            b->coef_off[i + 1] = b->coef_off[i] + size;
+            b->x_off[i + 1] = b->x_off[i] + nevals[i];
+            BuildArgs& a = p.args;
+            a.t = bl.tables;
+            a.r = bl.rhs;
+            a.raw = 0;
+            a.nlines = 1;
+            // offsets into the packed arrays, turned into pointers by the kernel
+            a.vals = reinterpret_cast<const double*>(intptr_t(b->vals_off[i]));
+            a.dlo = reinterpret_cast<const double*>(intptr_t(b->dlo_off[i]));
+            a.dhi = reinterpret_cast<const double*>(intptr_t(b->dhi_off[i]));
+            a.out = reinterpret_cast<double*>(intptr_t(b->coef_off[i]));
+            a.lv = Lines {np, 1, 1, 1, 0};
+            a.llo = Lines {bl.nbv_lo, 1, 1, 1, 0};
+            a.lhi = Lines {bl.nbv_hi, 1, 1, 1, 0};
+            a.lo = Lines {size, 1, 1, 1, 0};
+            a.pair16 = a.pair16_out = 0;
+            a.line_base = 0; // one line per problem, its arrays already offset
+            p.eb = ev.eb;
+            p.ex_lo = ev.ex_lo;
+            p.ex_hi = ev.ex_hi;
+            p.degree = ev.basis.desc.degree;
+            p.uniform = ev.basis.desc.uniform ? 1 : 0;
+            p.m = int(nevals[i]);
+            p.x_off = b->x_off[i];
+            p.out_off = b->x_off[i];
+            b->max_chunks = std::max(b->max_chunks, bl.tables.nchunk);
+            // a block's time on a problem: a fixed part (barriers, scans, the description) plus
+            // the rows and points its threads step through
+            cost[size_t(i)] = 64.0 + double(np) * (kShapes[p.shape][0] + kShapes[p.shape][1] + 2) / 8.0
+                              + double(nevals[i]) * (p.degree + 1) / 8.0;
+        }
+        // groups by band shape (splitting them further by tile size, so that short problems ask
+        // for less shared memory, measured slower: the groups' grids then balance worse); queue
+        // orders within each group
+        std::vector<int> order;
+        for (int sh = 0; sh < kNumShapes; ++sh) {
+            std::vector<int> members;
+            size_t smem = 0;
+            double c = 0.0;
+            for (int64_t i = 0; i < count; ++i) {
+                UnevenProblem const& p = probs[size_t(i)];
+                if (p.shape != sh) continue;
+                members.push_back(int(i));
+                smem = std::max(smem, problem_smem(p));
+                c += cost[size_t(i)];
+            }
+            if (members.empty()) continue;
+            b->gshape.push_back(sh);
+            b->gfirst.push_back(int(order.size() / 2));
+            b->gsize.push_back(int(members.size()));
+            b->gcost.push_back(c);
+            b->gsmem.push_back((smem + 15) & ~size_t(15));
+            b->smem = std::max(b->smem, b->gsmem.back());
+            std::vector<int> lpt = members;
+            std::stable_sort(lpt.begin(), lpt.end(), [&](int x, int y) { return cost[size_t(x)] > cost[size_t(y)]; });
+            order.insert(order.end(), lpt.begin(), lpt.end());
+            order.insert(order.end(), members.begin(), members.end());
+        }
+        if (count > 0) {
+            DDCB_CUDA_CHECK(cudaMalloc(&b->d_probs, sizeof(UnevenProblem) * size_t(count)));
+            DDCB_CUDA_CHECK(cudaMemcpy(b->d_probs, probs.data(), sizeof(UnevenProblem) * size_t(count), cudaMemcpyHostToDevice));
+            DDCB_CUDA_CHECK(cudaMalloc(&b->d_order, sizeof(int) * order.size()));
+            DDCB_CUDA_CHECK(cudaMemcpy(b->d_order, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice));
+        }
+        DDCB_CUDA_CHECK(cudaMalloc(&b->d_counter, sizeof(int) * std::max<size_t>(1, b->gshape.size())));
+        b->threads = std::max(256, (b->max_chunks + 31) / 32 * 32);
+        return b;
+    } catch (...) {
+        destroy_uneven_batch(b);
+        throw;
+    }
+}
+
+void destroy_uneven_batch(UnevenBatch* b)
+{
+    if (!b) return;
+    drop_graph(*b);
+    if (b->d_probs) cudaFree(b->d_probs);
+    if (b->d_order) cudaFree(b->d_order);
+    if (b->d_counter) cudaFree(b->d_counter);
+    delete b;
+}
+
+void uneven_offsets(UnevenBatch const& b, int64_t* vals, int64_t* dlo, int64_t* dhi, int64_t* coefs, int64_t* evals)
+{
+    auto copy = [&](std::vector<int64_t> const& v, int64_t* o) {
+        if (o) std::copy(v.begin(), v.end(), o);
+    };
+    copy(b.vals_off, vals);
+    copy(b.dlo_off, dlo);
+    copy(b.dhi_off, dhi);
+    copy(b.coef_off, coefs);
+    copy(b.x_off, evals);
+}
+
+void uneven_info(UnevenBatch const& b, int64_t* totals, int* schedule, double* tuned_us)
+{
+    totals[0] = b.count;
+    totals[1] = b.vals_off.back();
+    totals[2] = b.dlo_off.back();
+    totals[3] = b.dhi_off.back();
+    totals[4] = b.coef_off.back();
+    totals[5] = b.x_off.back();
+    schedule[0] = b.threads;
+    schedule[1] = b.blocks_per_sm;
+    schedule[2] = b.order;
+    schedule[3] = int(b.smem);
+    *tuned_us = b.tuned_us;
+}
+
+void run_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, double const* dhi, double* coefs,
+                      double const* coords, double* out, cudaStream_t s)
+{
+    if (b.count == 0) return;
+    UnevenArgs const key = make_args(b, 0, b.order, vals, dlo, dhi, coefs, coords, out);
+    bool const stale = !b.exec || key.vals != b.key.vals || key.dlo != b.key.dlo || key.dhi != b.key.dhi
+                       || key.coefs != b.key.coefs || key.coords != b.key.coords || key.out != b.key.out
+                       || s != b.key_stream || b.threads != b.key_threads || b.blocks_per_sm != b.key_blocks
+                       || b.order != b.key_order;
+    if (stale) {
+        drop_graph(b);
+        DDCB_CUDA_CHECK(cudaGraphCreate(&b.graph, 0));
+        cudaMemsetParams mp {};
+        mp.dst = b.d_counter;
+        mp.value = 0;
+        mp.elementSize = sizeof(int);
+        mp.width = b.gshape.size();
+        mp.height = 1;
+        mp.pitch = 0;
+        cudaGraphNode_t mnode = nullptr;
+        DDCB_CUDA_CHECK(cudaGraphAddMemsetNode(&mnode, b.graph, nullptr, 0, &mp));
+        for (int g = 0; g < int(b.gshape.size()); ++g) {
+            UnevenArgs args = make_args(b, g, b.order, vals, dlo, dhi, coefs, coords, out);
+            void* params[] = {&args};
+            cudaKernelNodeParams kp {};
+            kp.func = reinterpret_cast<void*>(kernel_of(b.gshape[size_t(g)]));
+            kp.gridDim = dim3(unsigned(group_blocks(b, g, b.threads, b.blocks_per_sm)));
+            kp.blockDim = dim3(unsigned(b.threads));
+            kp.sharedMemBytes = unsigned(b.gsmem[size_t(g)]);
+            kp.kernelParams = params;
+            cudaGraphNode_t knode = nullptr;
+            DDCB_CUDA_CHECK(cudaGraphAddKernelNode(&knode, b.graph, &mnode, 1, &kp));
+        }
+        DDCB_CUDA_CHECK(cudaGraphInstantiate(&b.exec, b.graph, 0));
+        b.key = key;
+        b.key_stream = s;
+        b.key_threads = b.threads;
+        b.key_blocks = b.blocks_per_sm;
+        b.key_order = b.order;
+    }
+    DDCB_CUDA_CHECK(cudaGraphLaunch(b.exec, s));
+}
+
+void tune_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, double const* dhi, double* coefs,
+                       double const* coords, double* out, int reps, cudaStream_t s)
+{
+    if (b.count == 0) return;
+    reps = std::max(1, reps);
+    cudaEvent_t e0, e1;
+    DDCB_CUDA_CHECK(cudaEventCreate(&e0));
+    DDCB_CUDA_CHECK(cudaEventCreate(&e1));
+    double best = 1e300;
+    int const t0 = b.threads, p0 = b.blocks_per_sm, o0 = b.order;
+    int bt = t0, bb = p0, bo = o0;
+    try {
+        // each candidate runs as the graph it would be launched as (the group kernels concurrent)
+        for (int threads : {128, 256, 512}) {
+            if (threads < b.max_chunks) continue; // one thread per chunk of the longest problem
+            for (int per : {1, 2, 3, 4, 6, 8}) {
+                for (int order : {0, 1}) {
+                    b.threads = threads;
+                    b.blocks_per_sm = per;
+                    b.order = order;
+                    run_uneven_batch(b, vals, dlo, dhi, coefs, coords, out, s); // builds the graph; warm-up
+                    DDCB_CUDA_CHECK(cudaEventRecord(e0, s));
+                    for (int r = 0; r < reps; ++r) run_uneven_batch(b, vals, dlo, dhi, coefs, coords, out, s);
+                    DDCB_CUDA_CHECK(cudaEventRecord(e1, s));
+                    DDCB_CUDA_CHECK(cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    DDCB_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+                    double const us = 1e3 * ms / reps;
+                    if (us < best) {
+                        best = us;
+                        bt = threads;
+                        bb = per;
+                        bo = order;
+                    }
+                }
+            }
+        }
+    } catch (...) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        b.threads = t0;
+        b.blocks_per_sm = p0;
+        b.order = o0;
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b.threads = bt;
+    b.blocks_per_sm = bb;
+    b.order = bo;
+    if (best < 1e300) b.tuned_us = best;
+}
+
+} // namespace ddcb

@@ -20,7 +20,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (EXTRAP_CONSTANT, EXTRAP_NULL, EXTRAP_PERIODIC, FP32_REFINE, FP64, GREVILLE, HERMITE,
-                   HOMOGENEOUS_HERMITE, PERIODIC, BuilderInfo, BuilderOptions, BSplinesInfo, Lines)
+                   HOMOGENEOUS_HERMITE, PERIODIC, BuilderInfo, BuilderOptions, BSplinesInfo, Lines, UnevenInfo)
 
 
 class SplineBuilderClosure:
@@ -422,5 +422,58 @@ class SplineEvaluator2D:
         nbatch = c[0, 0].numel()
         assert out.numel() == nbatch and out.is_contiguous() and c.is_contiguous()
         _lib.call("ddcb_integrate2d", self.evaluator1._h, self.evaluator2._h, _ptr(out), _ptr(c), int(nbatch),
+                  _stream_handle(stream))
+        return out
+
+
+class UnevenBatch:
+    """Many independent one-line problems (own builder and evaluator each) built and evaluated by
+    one graph launch of persistent kernels (ddcb_batch_uneven_*). Data are packed flat CUDA float64
+    arrays; `offsets()` gives every problem's slice. The builders and evaluators are kept alive by
+    the batch."""
+
+    def __init__(self, builders: Sequence[SplineBuilder], evaluators: Sequence[SplineEvaluator], nevals):
+        self.builders, self.evaluators = list(builders), list(evaluators)
+        n = len(self.builders)
+        bh = (C.c_void_p * max(n, 1))(*[b._h.value for b in self.builders])
+        eh = (C.c_void_p * max(n, 1))(*[e._h.value for e in self.evaluators])
+        ne = np.ascontiguousarray(nevals, dtype=np.int64)
+        h = C.c_void_p()
+        _lib.call("ddcb_batch_uneven_create", C.cast(bh, C.c_void_p), C.cast(eh, C.c_void_p),
+                  ne.ctypes.data_as(C.c_void_p), n, C.byref(h))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        L = getattr(_lib, "_lib", None) if _lib is not None else None
+        if h and L is not None:
+            L.ddcb_batch_uneven_destroy(h)
+            self._h = None
+
+    @property
+    def info(self) -> UnevenInfo:
+        info = UnevenInfo()
+        _lib.call("ddcb_batch_uneven_get_info", self._h, C.byref(info))
+        return info
+
+    def offsets(self):
+        n = len(self.builders) + 1
+        keys = ("vals", "derivs_lo", "derivs_hi", "coefs", "evals")
+        arrs = {k: np.zeros(n, dtype=np.int64) for k in keys}
+        _lib.call("ddcb_batch_uneven_offsets", self._h, *[arrs[k].ctypes.data_as(C.c_void_p) for k in keys])
+        return arrs
+
+    def _ptrs(self, vals, derivs_lo, derivs_hi, coefs, coords, out):
+        return [_ptr(_dev_f64(t, nm)) for t, nm in ((vals, "vals"), (derivs_lo, "derivs_lo"), (derivs_hi, "derivs_hi"),
+                                                    (coefs, "coefs"), (coords, "coords"), (out, "out"))]
+
+    def tune(self, vals, derivs_lo, derivs_hi, coefs, coords, out, reps: int = 3, stream=None):
+        """Time the candidate schedules on these buffers and keep the fastest (returns the info)."""
+        _lib.call("ddcb_batch_uneven_tune", self._h, *self._ptrs(vals, derivs_lo, derivs_hi, coefs, coords, out),
+                  int(reps), _stream_handle(stream))
+        return self.info
+
+    def __call__(self, vals, derivs_lo, derivs_hi, coefs, coords, out, stream=None):
+        _lib.call("ddcb_batch_uneven_run", self._h, *self._ptrs(vals, derivs_lo, derivs_hi, coefs, coords, out),
                   _stream_handle(stream))
         return out

@@ -92,3 +92,70 @@ def config3(nfields: int = 64, ncells: int = 512):
     coords = np.ascontiguousarray(np.stack([feet_x, feet_y], axis=-1))
     return dict(x=x, y=y, vals=np.ascontiguousarray(vals), dmin2=dmin2, dmax2=dmax2, coords=coords, ncells=ncells,
                 nfields=nfields)
+
+
+def config4(count: int = 4096, nmin: int = 32, nmax: int = 4096, seed: int = 0xDDC0 + 4):
+    """Uneven batch: `count` one-line problems, ncells log-uniform in [nmin, nmax], degree uniform in
+    1..5, closure uniform in {periodic, Hermite, Greville} (both ends), uniform or perturbed
+    (+-0.3 h) mesh on [0, 1], cos(2 pi k x + phi) samples (k in 1..8) with analytic Hermite
+    derivatives, evaluation at ncells uniform points per problem."""
+    u = splitmix_uniform(seed, 1, count)
+    nc = np.floor(np.exp(np.log(nmin) + u * (np.log(nmax + 1) - np.log(nmin)))).astype(np.int64)
+    nc = np.clip(nc, nmin, nmax)
+    deg = np.floor(splitmix_uniform(seed, 2, count) * 5).astype(np.int64) + 1
+    bc = np.floor(splitmix_uniform(seed, 3, count) * 3).astype(np.int64)  # 0 periodic, 1 Hermite, 2 Greville
+    uni = splitmix_uniform(seed, 4, count) < 0.5
+    k = np.floor(splitmix_uniform(seed, 5, count) * 8).astype(np.int64) + 1
+    ph = splitmix_uniform(seed, 6, count) * 2 * np.pi
+    probs = []
+    for i in range(count):
+        n = int(nc[i])
+        p = dict(ncells=n, degree=int(deg[i]), closure=("periodic", "hermite", "greville")[int(bc[i])],
+                 uniform=bool(uni[i]), k=int(k[i]), ph=float(ph[i]))
+        if not p["uniform"]:
+            h = 1.0 / n
+            br = np.arange(n + 1) * h
+            br[1:-1] += (splitmix_uniform(seed + i + 1, 7, n - 1) - 0.5) * 0.6 * h
+            br.sort()
+            br[0], br[-1] = 0.0, 1.0
+            p["breaks"] = br
+        p["coords"] = splitmix_uniform(seed + i + 1, 8, n)
+        probs.append(p)
+    return probs
+
+
+def config4_samples(p, points, nbv_lo, nbv_hi):
+    """Samples at the interpolation points and the Hermite derivatives (orders 1.. at each end)."""
+    vals = cos_family(points, p["k"], p["ph"])
+    lo = np.array([cos_family(0.0, p["k"], p["ph"], o) for o in range(1, nbv_lo + 1)])
+    hi = np.array([cos_family(1.0, p["k"], p["ph"], o) for o in range(1, nbv_hi + 1)])
+    return vals, lo, hi
+
+
+def config4_batch(D, probs):
+    """Builders, evaluators and packed host inputs (flat arrays in problem order) of config4
+    problems; `D` is the ddc_b200 package. Each builder solves one line: tile width 2 and about 16
+    rows per chunk."""
+    closure = {"periodic": 0, "hermite": 1, "greville": 3}
+    builders, evaluators, nevals = [], [], []
+    vals, dlo, dhi, coords = [], [], [], []
+    for p in probs:
+        n, d = p["ncells"], p["degree"]
+        per = p["closure"] == "periodic"
+        bs = D.UniformBSplines(d, per, 0.0, 1.0, n) if p["uniform"] else D.NonUniformBSplines(d, per, p["breaks"])
+        c = closure[p["closure"]]
+        b = D.SplineBuilder(bs, None, c, c, tile_lines=2, chunks=int(min(max(n // 16, 2), 256)))
+        e = D.SplineEvaluator(bs)
+        nlo = b.s_nbv_xmin if c == 1 else 0
+        nhi = b.s_nbv_xmax if c == 1 else 0
+        v, lo, hi = config4_samples(p, b.interpolation_points, nlo, nhi)
+        builders.append(b)
+        evaluators.append(e)
+        nevals.append(len(p["coords"]))
+        vals.append(v)
+        dlo.append(lo)
+        dhi.append(hi)
+        coords.append(p["coords"])
+    cat = lambda xs: np.ascontiguousarray(np.concatenate([np.asarray(x, dtype=np.float64).ravel() for x in xs]))
+    return dict(builders=builders, evaluators=evaluators, nevals=np.array(nevals, dtype=np.int64), vals=cat(vals),
+                dlo=cat(dlo), dhi=cat(dhi), coords=cat(coords))

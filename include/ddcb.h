@@ -196,6 +196,37 @@ ddcb_status ddcb_build_eval_adjoint(ddcb_builder b, ddcb_evaluator e, int32_t or
                                     double* g_derivs_hi, ddcb_lines g_derivs_hi_layout, double* g_coords,
                                     ddcb_lines g_coords_layout, int32_t* fused, ddcb_stream stream);
 
+/* ---- uneven batch: many independent one-line problems (each its own builder and evaluator:
+ *      size, degree, closure and mesh may all differ) built and evaluated by persistent kernels
+ *      in one CUDA graph launch (no reference counterpart: the reference loops one SplineBuilder
+ *      per problem). The builders and evaluators must outlive the batch and use FP64. Data are
+ *      packed: problem i's samples at vals[vals_off[i] .. vals_off[i+1]), its Hermite
+ *      derivatives likewise in derivs_lo / derivs_hi, its coefficients in coefs, and its
+ *      evaluation coordinates / values in coords / out at [evals_off[i] .. evals_off[i+1]). */
+typedef struct ddcb_uneven_batch_t* ddcb_uneven_batch;
+typedef struct ddcb_uneven_info {
+    int64_t count, total_vals, total_derivs_lo, total_derivs_hi, total_coefs, total_evals;
+    int32_t threads, blocks_per_sm, order, shared_bytes; /* the schedule in use (order 0: largest first) */
+    double tuned_us;                                     /* the tuner's best time (0: not tuned) */
+} ddcb_uneven_info;
+ddcb_status ddcb_batch_uneven_create(const ddcb_builder* builders, const ddcb_evaluator* evaluators,
+                                     const int64_t* nevals, int64_t count, ddcb_uneven_batch* out);
+ddcb_status ddcb_batch_uneven_destroy(ddcb_uneven_batch b);
+ddcb_status ddcb_batch_uneven_get_info(ddcb_uneven_batch b, ddcb_uneven_info* info);
+/* Prefix sums (count + 1 entries each; any pointer may be NULL). */
+ddcb_status ddcb_batch_uneven_offsets(ddcb_uneven_batch b, int64_t* vals_off, int64_t* derivs_lo_off,
+                                      int64_t* derivs_hi_off, int64_t* coefs_off, int64_t* evals_off);
+/* Times the candidate schedules (block size, blocks per SM, queue order), `reps` launches each, on
+ * these buffers and keeps the fastest for later runs. Overwrites coefs and out. */
+ddcb_status ddcb_batch_uneven_tune(ddcb_uneven_batch b, const double* vals, const double* derivs_lo,
+                                   const double* derivs_hi, double* coefs, const double* coords, double* out,
+                                   int32_t reps, ddcb_stream stream);
+/* Builds every problem and evaluates it at its coordinates (values, with its evaluator's boundary
+ * handling) in one graph launch. */
+ddcb_status ddcb_batch_uneven_run(ddcb_uneven_batch b, const double* vals, const double* derivs_lo,
+                                  const double* derivs_hi, double* coefs, const double* coords, double* out,
+                                  ddcb_stream stream);
+
 /* ---- 2D tensor product: SplineBuilder2D / SplineEvaluator2D on two 1D plans, for the layout
  *      (x1, x2, batch) with the batch contiguous (the reference's layout_right of
  *      DiscreteDomain<X1, X2, batch...>). ----------------------------------------------------- */
