@@ -47,6 +47,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--tile-lines", type=int, default=0, help="builder tile width (0 = plan default)")
     p.add_argument("--chunks", type=int, default=0, help="builder chunks per line (0 = plan default)")
+    p.add_argument("--no-configs", action="store_true", help="skip the other configurations' measurements")
     return p.parse_args()
 
 
@@ -187,6 +188,144 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def _time_ms(fn, reps, rotate=1):
+    """Mean CUDA-event time of fn(i) over `reps` calls after 3 warm-ups; i cycles over `rotate`
+    buffer sets (several sets larger than L2 in all keep each call's inputs out of L2)."""
+    import torch
+
+    for i in range(3):
+        fn(i % rotate)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(reps):
+        fn(i % rotate)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def measure_configs(peak, reps):
+    """The other configurations of the path, each at its named size (FP64 I/O, synthetic inputs):
+    periodic cubic 1000x1000 (build + evaluate), non-uniform quintic Hermite in FP32 + refinement,
+    the 2D periodic x Hermite cubic 512^2 x 64 fields, the uneven batch of 4096 problems, and the
+    differentiation step (forward and adjoint) on periodic cubic, 1024 cells x 65536 lines."""
+    import torch
+
+    import ddc_b200 as D
+    from ddc_b200 import workloads as W
+
+    dev = torch.device("cuda")
+    cu = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    out = {}
+    # ---- periodic uniform cubic, 1000 cells x 1000 lines, build + evaluate at 1000 points/line ----
+    w = W.config1()
+    bs = D.UniformBSplines(3, True, 0.0, 1.0, 1000)
+    b, e = D.SplineBuilder(bs), D.SplineEvaluator(bs)
+    sets = 8  # 8 x 40 MB > 2 x L2
+    vals = [cu(w["vals"]) for _ in range(sets)]
+    xs = [cu(w["coords"]) for _ in range(sets)]
+    cs = [torch.empty((bs.size, 1000), dtype=torch.float64, device=dev) for _ in range(sets)]
+    ys = [torch.empty((1000, 1000), dtype=torch.float64, device=dev) for _ in range(sets)]
+    fused = b.build_and_evaluate(e, cs[0], vals[0], xs[0], ys[0])
+    step = lambda i: b.build_and_evaluate(e, cs[i], vals[i], xs[i], ys[i])
+    ms_rot = _time_ms(step, 10 * reps, sets)
+    ms_l2 = _time_ms(step, 10 * reps, 1)
+    pts = 1000 * (1000 + 1000) / 2
+    bytes_fused = 1000 * 1000 * 8 + 1000 * 1003 * 8 + 1000 * 1000 * 16
+    out["periodic_cubic_1000x1000"] = {
+        "schedule": "fused build+eval kernel" if fused else "two kernels",
+        "ms": ms_rot, "Gpts_per_s": pts / ms_rot / 1e6, "GBps": bytes_fused / ms_rot / 1e6,
+        "hbm_frac": bytes_fused / ms_rot / 1e6 / peak, "ms_l2_resident": ms_l2,
+        "note": "8 rotating buffer sets (320 MB) for the HBM figure; one set for the L2-resident one"}
+    del vals, xs, cs, ys
+    # ---- non-uniform quintic Hermite, 65536 lines: FP64 vs FP32 + FP64 refinement -------------
+    br = W.config2_breaks(1024)
+    bs = D.NonUniformBSplines(5, False, br)
+    pts2 = D.greville_points(bs, 1, 1)
+    w = W.config2(B=1 << 16, points=pts2)
+    v, lo, hi = cu(w["vals"]), cu(w["dlo"]), cu(w["dhi"])
+    ref = torch.empty((bs.size, 1 << 16), dtype=torch.float64, device=dev)
+    b64 = D.SplineBuilder(bs, pts2, 1, 1)
+    t64 = _time_ms(lambda i: b64(ref, v, lo, hi), reps)
+    prec = {"fp64_build_ms": t64}
+    for rounds in (1, 2):
+        br_ = D.SplineBuilder(bs, pts2, 1, 1, precision="fp32_refine", refine_rounds=rounds)
+        c = torch.empty_like(ref)
+        t = _time_ms(lambda i: br_(c, v, lo, hi), reps)
+        err = float((c - ref).abs().max() / ref.abs().max())
+        prec[f"fp32_refine_{rounds}_rounds"] = {"build_ms": t, "speedup_vs_fp64": t64 / t, "max_rel_err_vs_fp64": err}
+    out["quintic_hermite_precision"] = prec
+    del v, lo, hi, ref
+    # ---- 2D: periodic cubic x Hermite cubic, 512 x 512, 64 fields ------------------------------
+    w = W.config3()
+    bx, by = D.UniformBSplines(3, True, 0.0, 1.0, 512), D.UniformBSplines(3, False, 0.0, 1.0, 512)
+    Bx, By = D.SplineBuilder(bx, None, 0, 0), D.SplineBuilder(by, None, 1, 1)
+    b2, e2 = D.SplineBuilder2D(Bx, By), D.SplineEvaluator2D(D.SplineEvaluator(bx), D.SplineEvaluator(by))
+    v, d0, d1, x = cu(w["vals"]), cu(w["dmin2"]), cu(w["dmax2"]), cu(w["coords"])
+    c2 = torch.empty((bx.size, by.size, 64), dtype=torch.float64, device=dev)
+    y2 = torch.empty(v.shape, dtype=torch.float64, device=dev)
+    tb = _time_ms(lambda i: b2(c2, v, derivs_min2=d0, derivs_max2=d1), reps)
+    te = _time_ms(lambda i: e2(y2, x, c2), reps)
+    n2 = v.numel()
+    b_bytes = (n2 + d0.numel() + d1.numel() + c2.numel()) * 8
+    e_bytes = (c2.numel() + 3 * n2) * 8
+    out["tensor2d_512x512x64"] = {"build_ms": tb, "eval_ms": te, "Gpts_per_s": n2 / (tb + te) / 1e6,
+                                  "build_GBps": b_bytes / tb / 1e6, "eval_GBps": e_bytes / te / 1e6,
+                                  "hbm_frac": (b_bytes + e_bytes) / (tb + te) / 1e6 / peak}
+    del v, d0, d1, x, c2, y2
+    # ---- uneven batch: 4096 problems ----------------------------------------------------------
+    probs = W.config4()
+    wb = W.config4_batch(D, probs)
+    batch = D.UnevenBatch(wb["builders"], wb["evaluators"], wb["nevals"])
+    info = batch.info
+    bv, blo, bhi, bx_ = cu(wb["vals"]), cu(wb["dlo"]), cu(wb["dhi"]), cu(wb["coords"])
+    bc = torch.empty((info.total_coefs,), dtype=torch.float64, device=dev)
+    by_ = torch.empty((info.total_evals,), dtype=torch.float64, device=dev)
+    tinf = batch.tune(bv, blo, bhi, bc, bx_, by_, reps=3)
+    tbatch = _time_ms(lambda i: batch(bv, blo, bhi, bc, bx_, by_), 10 * reps)
+    off = batch.offsets()
+    views = []
+    for i, (bb, ee) in enumerate(zip(wb["builders"], wb["evaluators"])):
+        sl = lambda t, k: t[off[k][i]:off[k][i + 1]][:, None]
+        views.append((bb, ee, sl(bv, "vals"), sl(blo, "derivs_lo") if off["derivs_lo"][i + 1] > off["derivs_lo"][i] else None,
+                      sl(bhi, "derivs_hi") if off["derivs_hi"][i + 1] > off["derivs_hi"][i] else None,
+                      sl(bc, "coefs"), sl(bx_, "evals"), sl(by_, "evals")))
+
+    def loop(i):
+        for bb, ee, vv, ll, hh, cc, xx, yy in views:
+            bb(cc, vv, ll, hh)
+            ee(yy, xx, cc)
+
+    tloop = _time_ms(loop, 2)
+    ub = 8 * (info.total_vals + info.total_derivs_lo + info.total_derivs_hi + info.total_coefs + 2 * info.total_evals)
+    out["uneven_batch_4096"] = {"problems": int(info.count), "points": int(info.total_vals), "evals": int(info.total_evals),
+                                "ms": tbatch, "Gpts_per_s": (info.total_vals + info.total_evals) / 2 / tbatch / 1e6,
+                                "GBps": ub / tbatch / 1e6, "loop_per_problem_fp64_ms": tloop, "speedup_vs_loop": tloop / tbatch,
+                                "schedule": {"threads": tinf.threads, "blocks_per_sm": tinf.blocks_per_sm,
+                                             "order": "largest-first" if tinf.order == 0 else "natural"}}
+    del batch, wb, views, bv, blo, bhi, bx_, bc, by_
+    # ---- differentiation: periodic cubic 1024 cells, 65536 lines, 1024 points/line ------------
+    B, m = 1 << 16, 1024
+    bs = D.UniformBSplines(3, True, 0.0, 1.0, 1024)
+    b, e = D.SplineBuilder(bs), D.SplineEvaluator(bs)
+    gen = torch.Generator(device=dev).manual_seed(5)
+    x = torch.rand((m, B), dtype=torch.float64, device=dev, generator=gen)
+    g = torch.randn((m, B), dtype=torch.float64, device=dev, generator=gen)
+    v = torch.randn((1024, B), dtype=torch.float64, device=dev, generator=gen)
+    c = torch.empty((1027, B), dtype=torch.float64, device=dev)
+    y = torch.empty((m, B), dtype=torch.float64, device=dev)
+    gv = torch.empty((1024, B), dtype=torch.float64, device=dev)
+    gx = torch.empty((m, B), dtype=torch.float64, device=dev)
+    tf = _time_ms(lambda i: b.build_and_evaluate(e, c, v, x, y), reps)
+    tb_ = _time_ms(lambda i: b.build_and_evaluate_adjoint(e, x, c, g, gv, gx), reps)
+    fwd_bytes = B * (1024 + 1027 + 2 * m) * 8
+    bwd_bytes = B * (m + m + 1027 + m + 1024) * 8
+    out["adjoint_periodic_cubic_1024x65536"] = {"fwd_ms": tf, "bwd_ms": tb_, "fwd_GBps": fwd_bytes / tf / 1e6,
+                                                "bwd_GBps": bwd_bytes / tb_ / 1e6, "bwd_hbm_frac": bwd_bytes / tb_ / 1e6 / peak}
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -298,15 +437,22 @@ def run_ours(args):
     e2e_value = total_pts / (e_ms_total / ke * 1e-3) / 1e9
     h2d = sum(t.numel() * 8 for t in (h_vals, h_dlo, h_dhi, h_x))
     d2h = h_out.numel() * 8
-    # ---- roofline of the dominant kernel (the fused build + derivative kernel) ----
+    # ---- roofline of the dominant kernel: the fused build + derivative kernel when the step ran
+    # as one kernel, else the longer of the builder and evaluator kernels ----
     b_bytes, e_bytes = algorithmic_bytes(lines, npts, 4, bs.size, m)
     f_bytes = b_bytes + lines * m * 16  # coefficients written once, never re-read
     peak, peak_kind = peaks()
-    achieved = f_bytes / (f_ms * 1e-3) / 1e9
+    if fused:
+        kname, kbytes, kms, kkey = "build_eval_kernel (fused build + deriv)", f_bytes, f_ms, "build_eval_kernel"
+    elif e_ms >= b_ms:
+        kname, kbytes, kms, kkey = "eval_kernel (first derivative)", e_bytes, e_ms, "eval_kernel"
+    else:
+        kname, kbytes, kms, kkey = "build_kernel", b_bytes, b_ms, "build_kernel"
+    achieved = kbytes / (kms * 1e-3) / 1e9
     traffic = None
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            traffic = json.load(f).get("build_eval_fused")
+            traffic = json.load(f).get(kkey)
     except Exception:
         pass
     result = None
@@ -329,13 +475,13 @@ def run_ours(args):
                                    "points per line",
                        "lines_per_gpu": lines, "degree": 5, "ncells": 1024, "eval_points_per_line": m,
                        "l2": "inputs larger than L2 (2.2 GB touched per step)",
-                       "schedule": "fused build+deriv kernel" if fused else "two kernels",
+                       "schedule": "fused build+deriv kernel" if fused else "builder kernel then evaluator kernel",
                        "parallelism": f"batch-sharded x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "kernel": "build_eval_kernel (fused)",
-                         "algorithmic_bytes_per_launch": f_bytes, "peak_kind": peak_kind},
-            "kernels": {"fused_ms": f_ms, "fused_GBps": achieved,
-                        "two_call": {"build_ms": b_ms, "eval_ms": e_ms,
+                         "frac": achieved / peak, "traffic": traffic, "kernel": kname,
+                         "algorithmic_bytes_per_launch": kbytes, "peak_kind": peak_kind},
+            "kernels": {"step_ms": f_ms, "step_algorithmic_GBps": (f_bytes if fused else b_bytes + e_bytes) / (f_ms * 1e-3) / 1e9,
+                        "per_kernel": {"build_ms": b_ms, "eval_ms": e_ms,
                                      "build_GBps": b_bytes / (b_ms * 1e-3) / 1e9,
                                      "eval_GBps": e_bytes / (e_ms * 1e-3) / 1e9,
                                      "Gpts_per_s": total_pts / ((b_ms + e_ms) * 1e-3) / 1e9 / world}},
@@ -345,6 +491,11 @@ def run_ours(args):
             "gpu_launches": args.steps if fused else 2 * args.steps,
             "clocks": clk,
         }
+        if not args.no_configs and world == 1:
+            try:
+                result["configs"] = measure_configs(peak, max(3, args.steps // 2))
+            except Exception as exc:  # reported, not required for the headline line
+                result["configs"] = {"error": f"{type(exc).__name__}: {exc}"}
         print(json.dumps(result), flush=True)
     if world > 1:
         dist.barrier()

@@ -78,11 +78,14 @@ bool launch5(BuildArgs const& args, FusedEval const& fe, cudaStream_t s)
     return true;
 }
 
+// Uniform bases only: on non-uniform meshes the evaluator kernel alone (its own block shape for
+// the table lookups) after the builder measured faster than one fused kernel.
 template <int KL, int KU, int D>
 bool launch_ord(BuildArgs const& args, FusedEval const& fe, int order, bool uni, cudaStream_t s)
 {
-    if (order == 0) return uni ? launch5<KL, KU, D, 0, true>(args, fe, s) : launch5<KL, KU, D, 0, false>(args, fe, s);
-    if (order == 1) return uni ? launch5<KL, KU, D, 1, true>(args, fe, s) : launch5<KL, KU, D, 1, false>(args, fe, s);
+    if (!uni) return false;
+    if (order == 0) return launch5<KL, KU, D, 0, true>(args, fe, s);
+    if (order == 1) return launch5<KL, KU, D, 1, true>(args, fe, s);
     return false;
 }
 
