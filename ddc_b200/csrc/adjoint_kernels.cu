@@ -70,54 +70,109 @@ struct AdjointArgs
     Lines lglo;
     double* gdhi;
     Lines lghi;
+    int pair_in;            // g_coefs: adjacent line pairs 16-byte aligned and contiguous
+    int pair_out;           // g_vals: the same
 };
 
 // P^T: tile row j (column j of the solve) collects the cotangents of every coefficient row b with
-// coef_row(b) = j, i.e. b = (j + srot) mod n, + n, ... below size. Ends with a barrier.
+// coef_row(b) = j, i.e. b = (j + srot) mod n, + n, ... below size. The first occurrence of each
+// row arrives by async copies (two lines per 16-byte copy where aligned); the few periodic
+// duplicates (rows n .. size-1) are added after. Ends with a barrier.
 template <int TL>
 __device__ __forceinline__ void gather_adjoint(AdjointArgs const& a, double* T)
 {
     int const n = a.t.n;
     int const size = a.r.size;
     int const tid = threadIdx.x;
-    int const l = tid % TL;
-    int const c = tid / TL;
-    int64_t const line = (int64_t)blockIdx.x * TL + l;
-    bool const live = line < a.nlines;
-    int64_t const og = live ? line_offset(a.lgc, line) : 0;
-    for (int j = c; j < n; j += a.nct) {
-        double v = 0.0;
-        if (live) {
+    if (TL % 2 == 0 && a.pair_in) {
+        int const p = tid % (TL / 2);
+        int const c2 = tid / (TL / 2);
+        int const step = blockDim.x / (TL / 2);
+        int64_t const line = (int64_t)blockIdx.x * TL + 2 * p;
+        bool const live0 = line < a.nlines, live1 = line + 1 < a.nlines;
+        int64_t const og = live0 ? line_offset(a.lgc, line) : 0;
+        for (int j = c2; j < n; j += step) {
             int b = j + a.r.srot;
             b -= (b >= n) ? n : 0;
-            for (; b < size; b += n) v += a.gc[b * a.lgc.stride + og];
+            double* dst = T + j * TL + 2 * p;
+            if (live1) cp_async16(dst, a.gc + b * a.lgc.stride + og);
+            else {
+                dst[0] = live0 ? a.gc[b * a.lgc.stride + og] : 0.0;
+                dst[1] = 0.0;
+            }
         }
-        T[j * TL + l] = v;
+    } else {
+        int const l = tid % TL;
+        int const c = tid / TL;
+        int64_t const line = (int64_t)blockIdx.x * TL + l;
+        bool const live = line < a.nlines;
+        int64_t const og = live ? line_offset(a.lgc, line) : 0;
+        for (int j = c; j < n; j += a.nct) {
+            int b = j + a.r.srot;
+            b -= (b >= n) ? n : 0;
+            if (live) cp_async8(T + j * TL + l, a.gc + b * a.lgc.stride + og);
+            else T[j * TL + l] = 0.0;
+        }
     }
+    cp_async_wait_all();
     __syncthreads();
+    if (size > n) {
+        int const l = tid % TL;
+        int const c = tid / TL;
+        int64_t const line = (int64_t)blockIdx.x * TL + l;
+        if (line < a.nlines) {
+            int64_t const og = line_offset(a.lgc, line);
+            for (int b = n + c; b < size; b += a.nct) {
+                int j = (b - n) - a.r.srot; // row of the first occurrence, b - n
+                j += (j < 0) ? n : 0;
+                T[j * TL + l] += a.gc[b * a.lgc.stride + og];
+            }
+        }
+        __syncthreads();
+    }
 }
 
 // R^T: tile row i of the transposed solve is the cotangent of system row (i + lrot) mod n: a
-// sample, or a Hermite derivative (times the dx^k the forward pass scaled it by).
+// sample, or a Hermite derivative (times the dx^k the forward pass scaled it by). Samples leave by
+// streaming stores, two lines per 16-byte store where aligned.
 template <int TL>
 __device__ __forceinline__ void store_adjoint(AdjointArgs const& a, const double* T)
 {
     RhsMap const& R = a.r;
     int const n = a.t.n;
     int const tid = threadIdx.x;
+    int const v0 = R.periodic ? 0 : R.nbe_lo;
+    int const v1 = R.periodic ? n : R.nbe_lo + R.npoints;
+    if (TL % 2 == 0 && a.pair_out) {
+        int const p = tid % (TL / 2);
+        int const c2 = tid / (TL / 2);
+        int const step = blockDim.x / (TL / 2);
+        int64_t const line = (int64_t)blockIdx.x * TL + 2 * p;
+        if (line < a.nlines) {
+            bool const live1 = line + 1 < a.nlines;
+            int64_t const ov = line_offset(a.lgv, line);
+            for (int i = c2; i < n; i += step) {
+                int sr = i + R.lrot;
+                sr -= (sr >= n) ? n : 0;
+                if (sr < v0 || sr >= v1) continue;
+                double2 const g = *reinterpret_cast<const double2*>(T + i * TL + 2 * p);
+                double* dst = a.gv + (int64_t)(sr - v0) * a.lgv.stride + ov;
+                if (live1) __stcs(reinterpret_cast<double2*>(dst), g);
+                else __stcs(dst, g.x);
+            }
+        }
+    }
     int const l = tid % TL;
     int const c = tid / TL;
     int64_t const line = (int64_t)blockIdx.x * TL + l;
     if (line >= a.nlines) return;
-    int const v0 = R.periodic ? 0 : R.nbe_lo;
-    int const v1 = R.periodic ? n : R.nbe_lo + R.npoints;
     int64_t const ov = line_offset(a.lgv, line);
     for (int i = c; i < n; i += a.nct) {
         int sr = i + R.lrot;
         sr -= (sr >= n) ? n : 0;
         double const g = T[i * TL + l];
         if (sr >= v0 && sr < v1) {
-            a.gv[(int64_t)(sr - v0) * a.lgv.stride + ov] = g;
+            if (!(TL % 2 == 0 && a.pair_out)) __stcs(a.gv + (int64_t)(sr - v0) * a.lgv.stride + ov, g);
         } else if (sr < v0) {
             if (sr < R.nbv_lo && a.gdlo) a.gdlo[sr * a.lglo.stride + line_offset(a.lglo, line)] = g * R.dxpow_lo[sr];
         } else {
@@ -426,6 +481,8 @@ AdjointArgs make_adjoint_args(Builder const& b, const double* gc, Lines const& l
     a.lglo = lglo;
     a.gdhi = gdhi;
     a.lghi = lghi;
+    a.pair_in = gc != nullptr && line_pairs_aligned(gc, lgc);
+    a.pair_out = line_pairs_aligned(gv, lgv);
     return a;
 }
 
