@@ -48,6 +48,8 @@ def parse():
     p.add_argument("--tile-lines", type=int, default=0, help="builder tile width (0 = plan default)")
     p.add_argument("--chunks", type=int, default=0, help="builder chunks per line (0 = plan default)")
     p.add_argument("--no-configs", action="store_true", help="skip the other configurations' measurements")
+    p.add_argument("--profile-case", choices=["adjoint", "periodic_cubic", "tensor2d"], default=None,
+                   help="run only this case's kernels, --steps times on --lines lines (for profilers; prints no JSON line)")
     return p.parse_args()
 
 
@@ -503,8 +505,53 @@ def run_ours(args):
     return result
 
 
+def profile_case(args):
+    """A short run of one case's kernels at a chosen batch, for ncu captures on small workloads:
+    adjoint = periodic cubic 1024 cells, build + evaluate then its backward; periodic_cubic = the
+    fused build + evaluate of 1000 cells; tensor2d = the 2D build and evaluation of 512 x 512 cells
+    over --lines fields."""
+    import torch
+
+    import ddc_b200 as D
+    from ddc_b200 import workloads as W
+
+    dev = torch.device("cuda")
+    B = args.lines
+    gen = torch.Generator(device=dev).manual_seed(5)
+    if args.profile_case in ("adjoint", "periodic_cubic"):
+        n = 1024 if args.profile_case == "adjoint" else 1000
+        bs = D.UniformBSplines(3, True, 0.0, 1.0, n)
+        b, e = D.SplineBuilder(bs), D.SplineEvaluator(bs)
+        x = torch.rand((n, B), dtype=torch.float64, device=dev, generator=gen)
+        v = torch.randn((n, B), dtype=torch.float64, device=dev, generator=gen)
+        g = torch.randn((n, B), dtype=torch.float64, device=dev, generator=gen)
+        c = torch.empty((bs.size, B), dtype=torch.float64, device=dev)
+        y = torch.empty((n, B), dtype=torch.float64, device=dev)
+        gv, gx = torch.empty_like(v), torch.empty_like(x)
+        for _ in range(args.steps):
+            b.build_and_evaluate(e, c, v, x, y)
+            if args.profile_case == "adjoint":
+                b.build_and_evaluate_adjoint(e, x, c, g, gv, gx)
+    else:
+        w = W.config3(nfields=B)
+        cu = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        bx, by = D.UniformBSplines(3, True, 0.0, 1.0, 512), D.UniformBSplines(3, False, 0.0, 1.0, 512)
+        b2 = D.SplineBuilder2D(D.SplineBuilder(bx, None, 0, 0), D.SplineBuilder(by, None, 1, 1))
+        e2 = D.SplineEvaluator2D(D.SplineEvaluator(bx), D.SplineEvaluator(by))
+        v, d0, d1, x = cu(w["vals"]), cu(w["dmin2"]), cu(w["dmax2"]), cu(w["coords"])
+        c2 = torch.empty((bx.size, by.size, B), dtype=torch.float64, device=dev)
+        y2 = torch.empty(v.shape, dtype=torch.float64, device=dev)
+        for _ in range(args.steps):
+            b2(c2, v, derivs_min2=d0, derivs_max2=d1)
+            e2(y2, x, c2)
+    torch.cuda.synchronize()
+
+
 def main():
     args = parse()
+    if args.profile_case:
+        profile_case(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
