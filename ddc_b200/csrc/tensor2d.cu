@@ -29,10 +29,12 @@ int64_t group_fields(Builder const& b1, Builder const& b2, int64_t nbatch)
 
 } // namespace
 
+// Workspace: the x1 results of one group of fields over the values, (s1, np2, G), then the x1
+// results of the dim-2 derivative slabs of every field, (s1, nlo2, B) and (s1, nhi2, B).
 size_t build2d_workspace_bytes(Builder const& b1, Builder const& b2, int64_t nbatch)
 {
     int64_t const G = group_fields(b1, b2, nbatch);
-    return size_t(b1.basis.size()) * size_t(b2.points.size() + b2.nbv_lo + b2.nbv_hi) * size_t(G) * 8;
+    return size_t(b1.basis.size()) * (size_t(b2.points.size()) * size_t(G) + size_t(b2.nbv_lo + b2.nbv_hi) * size_t(nbatch)) * 8;
 }
 
 void launch_build2d(Builder const& b1, Builder const& b2, double* coefs, double const* vals, double const* dmin1,
@@ -45,36 +47,34 @@ void launch_build2d(Builder const& b1, Builder const& b2, double* coefs, double 
     bool const her_lo2 = b2.lo == DDCB_HERMITE && nlo2 > 0, her_hi2 = b2.hi == DDCB_HERMITE && nhi2 > 0;
     int64_t const G0 = group_fields(b1, b2, B);
     Lines const none {0, 1, 0, 0, 0};
+    double* S1 = ws;                        // (s1, np2, G0): one group's x1 pass over the values
+    double* S1lo = S1 + s1 * np2 * G0;      // (s1, nlo2, B): every field's lower derivative slab
+    double* S1hi = S1lo + s1 * nlo2 * B;    // (s1, nhi2, B)
+    // lines of an x1 pass over an (x1, q, ld) array, for G fields: (q, field)
+    auto x1_lines = [&](int64_t n, int64_t nq, int64_t ld, int64_t G) { return Lines {n, nq * ld, G, nq, ld}; };
+    // (a), (c) x1 passes over the dim-2 derivative slabs of all fields at once (a few rows per field:
+    // one launch each instead of one per group), with the mixed derivatives as Hermite data
+    if (her_lo2) {
+        launch_build(b1, S1lo, x1_lines(s1, nlo2, B, B), dmin2, x1_lines(np1, nlo2, B, B), m11,
+                     m11 ? x1_lines(nlo1, nlo2, B, B) : none, m21, m21 ? x1_lines(nhi1, nlo2, B, B) : none, s);
+    }
+    if (her_hi2) {
+        launch_build(b1, S1hi, x1_lines(s1, nhi2, B, B), dmax2, x1_lines(np1, nhi2, B, B), m12,
+                     m12 ? x1_lines(nlo1, nhi2, B, B) : none, m22, m22 ? x1_lines(nhi1, nhi2, B, B) : none, s);
+    }
     for (int64_t f0 = 0; f0 < B; f0 += G0) {
         int64_t const G = std::min(G0, B - f0);
-        double* S1 = ws;                       // (s1, np2, G)
-        double* S1lo = S1 + s1 * np2 * G;      // (s1, nlo2, G)
-        double* S1hi = S1lo + s1 * nlo2 * G;   // (s1, nhi2, G)
-        // lines of an x1 pass over an (x1, q, B) array restricted to the group: (q, field)
-        auto x1_lines = [&](int64_t n, int64_t nq, int64_t ld) { return Lines {n, nq * ld, G, nq, ld}; };
-        // (a) x1 pass over the lower dim-2 derivative slab, with the mixed derivatives as Hermite data
-        if (her_lo2) {
-            launch_build(b1, S1lo, x1_lines(s1, nlo2, G), dmin2 + f0, x1_lines(np1, nlo2, B), m11 ? m11 + f0 : nullptr,
-                               m11 ? x1_lines(nlo1, nlo2, B) : none, m21 ? m21 + f0 : nullptr,
-                               m21 ? x1_lines(nhi1, nlo2, B) : none, s);
-        }
-        // (b) x1 pass over the values
-        launch_build(b1, S1, x1_lines(s1, np2, G), vals + f0, x1_lines(np1, np2, B), dmin1 ? dmin1 + f0 : nullptr,
-                           dmin1 ? x1_lines(nlo1, np2, B) : none, dmax1 ? dmax1 + f0 : nullptr,
-                           dmax1 ? x1_lines(nhi1, np2, B) : none, s);
-        // (c) x1 pass over the upper dim-2 derivative slab
-        if (her_hi2) {
-            launch_build(b1, S1hi, x1_lines(s1, nhi2, G), dmax2 + f0, x1_lines(np1, nhi2, B), m12 ? m12 + f0 : nullptr,
-                               m12 ? x1_lines(nlo1, nhi2, B) : none, m22 ? m22 + f0 : nullptr,
-                               m22 ? x1_lines(nhi1, nhi2, B) : none, s);
-        }
+        // (b) x1 pass over the values of the group
+        launch_build(b1, S1, x1_lines(s1, np2, G, G), vals + f0, x1_lines(np1, np2, B, G), dmin1 ? dmin1 + f0 : nullptr,
+                     dmin1 ? x1_lines(nlo1, np2, B, G) : none, dmax1 ? dmax1 + f0 : nullptr,
+                     dmax1 ? x1_lines(nhi1, np2, B, G) : none, s);
         // (d) x2 pass: lines (row r of the x1 coefficients, field) of the x1 results
         Lines const lv2 {np2, G, G, s1, np2 * G};
-        Lines const llo2 {nlo2, G, G, s1, nlo2 * G};
-        Lines const lhi2 {nhi2, G, G, s1, nhi2 * G};
+        Lines const llo2 {nlo2, B, G, s1, nlo2 * B};
+        Lines const lhi2 {nhi2, B, G, s1, nhi2 * B};
         Lines const lc2 {s2, B, G, s1, s2 * B};
-        launch_build(b2, coefs + f0, lc2, S1, lv2, her_lo2 ? S1lo : nullptr, her_lo2 ? llo2 : none,
-                           her_hi2 ? S1hi : nullptr, her_hi2 ? lhi2 : none, s);
+        launch_build(b2, coefs + f0, lc2, S1, lv2, her_lo2 ? S1lo + f0 : nullptr, her_lo2 ? llo2 : none,
+                     her_hi2 ? S1hi + f0 : nullptr, her_hi2 ? lhi2 : none, s);
     }
 }
 
