@@ -151,6 +151,47 @@ __device__ __forceinline__ void nonuniform_values_span2(const double* kn, const 
     }
 }
 
+// Non-uniform Cox-de Boor values of degree P on the cell whose knots are kn (the layout of
+// nonuniform_values_span), dividing by the knot differences themselves: the j+1 denominators of
+// level j are inverted together with one division (prefix products, then one reciprocal, then
+// back-substitution of the products). Empty spans (repeated boundary knots) contribute 0. The
+// products hold at most P knot differences, so they stay in FP64 range for spacings between
+// 1e-60 and 1e60 of the coordinate unit.
+template <int P>
+__device__ __forceinline__ void nonuniform_values_div(const double* kn, double x, double* v)
+{
+    double left[P + 1], right[P + 1];
+    v[0] = 1.0;
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+        left[j] = x - kn[P - 1 - j];
+        right[j] = kn[P + j] - x;
+        double d[P], pre[P], inv_d[P];
+#pragma unroll
+        for (int r = 0; r <= j; ++r) {
+            double const den = kn[P + r] - kn[P - 1 - j + r];
+            d[r] = den != 0.0 ? den : 1.0;
+            pre[r] = r == 0 ? d[0] : pre[r - 1] * d[r];
+        }
+        double inv = 1.0 / pre[j];
+#pragma unroll
+        for (int r = j; r >= 1; --r) {
+            inv_d[r] = inv * pre[r - 1];
+            inv *= d[r];
+        }
+        inv_d[0] = inv;
+        double saved = 0.0;
+#pragma unroll
+        for (int r = 0; r < j + 1; ++r) {
+            double const den = kn[P + r] - kn[P - 1 - j + r];
+            double const temp = den != 0.0 ? v[r] * inv_d[r] : 0.0;
+            v[r] = saved + right[r] * temp;
+            saved = left[j - r] * temp;
+        }
+        v[j + 1] = saved;
+    }
+}
+
 // s(x) without boundary handling (spline_evaluator.hpp:556-605).
 template <int D, bool UNI, class Acc>
 __device__ __forceinline__ double eval_value_no_bc(EvalBasis const& eb, double x, Acc const& C)
@@ -205,6 +246,41 @@ __device__ __forceinline__ double eval_deriv_no_bc(EvalBasis const& eb, double x
     double cc[D + 1];
     double v[P + 1];
     int jmin;
+    if constexpr (!UNI && ORDER == 1) {
+        // first derivative on a non-uniform mesh: the 2D knots around the cell give both the
+        // degree-(D-1) basis and the divided-difference factors D / (t[jmin+i+D] - t[jmin+i]),
+        // computed here instead of read from the span table
+        int const ck = nonuniform_locate(eb, x);
+        jmin = ck - D;
+        double kn[2 * D]; // t[ck-D+1 .. ck+D]
+        load_knots<D>(eb, ck, kn);
+        if constexpr (P > 0) nonuniform_values_div<P>(kn + 1, x, v);
+        else v[0] = 1.0;
+        double d[D], pre[D], f[D + 1];
+#pragma unroll
+        for (int i = 1; i <= D; ++i) {
+            double const den = kn[D - 1 + i] - kn[i - 1];
+            d[i - 1] = den != 0.0 ? den : 1.0;
+            pre[i - 1] = i == 1 ? d[0] : pre[i - 2] * d[i - 1];
+        }
+        double inv = double(D) / pre[D - 1];
+#pragma unroll
+        for (int i = D; i >= 2; --i) {
+            f[i] = inv * pre[i - 2];
+            inv *= d[i - 1];
+        }
+        f[1] = inv;
+        int const r0 = C.row0(jmin);
+#pragma unroll
+        for (int i = 0; i < D + 1; ++i) cc[i] = C.get(r0, i);
+        double y = 0.0;
+#pragma unroll
+        for (int r = 0; r < P + 1; ++r) {
+            double const den = kn[D + r] - kn[r];
+            y = fma(den != 0.0 ? (cc[r + 1] - cc[r]) * f[r + 1] : 0.0, v[r], y);
+        }
+        return y;
+    }
     if (UNI) {
         double off;
         jmin = uniform_cell(eb.b, x, off);
