@@ -2,9 +2,9 @@
 //
 // Uniform bases need no tables: the cell comes from a scaled offset and the basis from the
 // uniform Cox-de Boor triangle. Non-uniform bases read the knots around the cell as (t_i, t_i+1)
-// pairs from shared memory (16-byte loads) and the knot-span inverses the Cox-de Boor triangle and
-// the derivative differences need from a small table built with the evaluator (L1-resident), so
-// the device evaluation divides nothing.
+// pairs from shared memory (16-byte loads). Values and first derivatives divide by the knot
+// differences, one division per level of the triangle (batched inversion); higher derivatives and
+// the adjoints take the knot-span inverses from a small table built with the evaluator.
 #pragma once
 
 #include "bspline_math.cuh"
@@ -155,8 +155,8 @@ __device__ __forceinline__ void nonuniform_values_span2(const double* kn, const 
 // nonuniform_values_span), dividing by the knot differences themselves: the j+1 denominators of
 // level j are inverted together with one division (prefix products, then one reciprocal, then
 // back-substitution of the products). Empty spans (repeated boundary knots) contribute 0. The
-// products hold at most P knot differences, so they stay in FP64 range for spacings between
-// 1e-60 and 1e60 of the coordinate unit.
+// products hold at most P knot differences, so they stay in FP64 range for spacings between 1e-60
+// and 1e60 of the coordinate unit.
 template <int P>
 __device__ __forceinline__ void nonuniform_values_div(const double* kn, double x, double* v)
 {
@@ -170,7 +170,7 @@ __device__ __forceinline__ void nonuniform_values_div(const double* kn, double x
 #pragma unroll
         for (int r = 0; r <= j; ++r) {
             double const den = kn[P + r] - kn[P - 1 - j + r];
-            d[r] = den != 0.0 ? den : 1.0;
+            d[r] = den == 0.0 ? 1.0 : den;
             pre[r] = r == 0 ? d[0] : pre[r - 1] * d[r];
         }
         double inv = 1.0 / pre[j];
@@ -183,13 +183,53 @@ __device__ __forceinline__ void nonuniform_values_div(const double* kn, double x
         double saved = 0.0;
 #pragma unroll
         for (int r = 0; r < j + 1; ++r) {
-            double const den = kn[P + r] - kn[P - 1 - j + r];
-            double const temp = den != 0.0 ? v[r] * inv_d[r] : 0.0;
+            double temp = v[r] * inv_d[r];
+            if (kn[P + r] == kn[P - 1 - j + r]) temp = 0.0;
             v[r] = saved + right[r] * temp;
             saved = left[j - r] * temp;
         }
         v[j + 1] = saved;
     }
+}
+
+// s'(x) on the non-uniform cell ck (spline_evaluator.hpp:357-478 for order 1): the 2D knots around
+// the cell give both the degree-(D-1) basis and the divided-difference factors
+// D / (t[jmin+i+D] - t[jmin+i]), computed here rather than read from the span table.
+template <int D, class Acc>
+__device__ __forceinline__ double nonuniform_deriv1(EvalBasis const& eb, int ck, double x, Acc const& C)
+{
+    constexpr int P = D - 1;
+    double kn[2 * D]; // t[ck-D+1 .. ck+D]
+    load_knots<D>(eb, ck, kn);
+    double v[P + 1];
+    if constexpr (P > 0) nonuniform_values_div<P>(kn + 1, x, v);
+    else v[0] = 1.0;
+    double d[D], pre[D], f[D + 1];
+#pragma unroll
+    for (int i = 1; i <= D; ++i) {
+        double const den = kn[D - 1 + i] - kn[i - 1];
+        d[i - 1] = den == 0.0 ? 1.0 : den;
+        pre[i - 1] = i == 1 ? d[0] : pre[i - 2] * d[i - 1];
+    }
+    double inv = double(D) / pre[D - 1];
+#pragma unroll
+    for (int i = D; i >= 2; --i) {
+        f[i] = inv * pre[i - 2];
+        inv *= d[i - 1];
+    }
+    f[1] = inv;
+    int const r0 = C.row0(ck - D);
+    double y = 0.0;
+    double cprev = C.get(r0, 0);
+#pragma unroll
+    for (int r = 0; r < P + 1; ++r) {
+        double const ci = C.get(r0, r + 1);
+        double a = (ci - cprev) * f[r + 1];
+        if (kn[D + r] == kn[r]) a = 0.0;
+        y = fma(a, v[r], y);
+        cprev = ci;
+    }
+    return y;
 }
 
 // s(x) without boundary handling (spline_evaluator.hpp:556-605).
@@ -207,7 +247,7 @@ __device__ __forceinline__ double eval_value_no_bc(EvalBasis const& eb, double x
         jmin = ck - D;
         double kn[2 * D];
         load_knots<D>(eb, ck, kn);
-        nonuniform_values_span<D>(kn, eb.inv_span + ck, eb.nk, x, v);
+        nonuniform_values_div<D>(kn, x, v);
     }
     int const r0 = C.row0(jmin);
     double y = 0.0;
@@ -247,39 +287,8 @@ __device__ __forceinline__ double eval_deriv_no_bc(EvalBasis const& eb, double x
     double v[P + 1];
     int jmin;
     if constexpr (!UNI && ORDER == 1) {
-        // first derivative on a non-uniform mesh: the 2D knots around the cell give both the
-        // degree-(D-1) basis and the divided-difference factors D / (t[jmin+i+D] - t[jmin+i]),
-        // computed here instead of read from the span table
         int const ck = nonuniform_locate(eb, x);
-        jmin = ck - D;
-        double kn[2 * D]; // t[ck-D+1 .. ck+D]
-        load_knots<D>(eb, ck, kn);
-        if constexpr (P > 0) nonuniform_values_div<P>(kn + 1, x, v);
-        else v[0] = 1.0;
-        double d[D], pre[D], f[D + 1];
-#pragma unroll
-        for (int i = 1; i <= D; ++i) {
-            double const den = kn[D - 1 + i] - kn[i - 1];
-            d[i - 1] = den != 0.0 ? den : 1.0;
-            pre[i - 1] = i == 1 ? d[0] : pre[i - 2] * d[i - 1];
-        }
-        double inv = double(D) / pre[D - 1];
-#pragma unroll
-        for (int i = D; i >= 2; --i) {
-            f[i] = inv * pre[i - 2];
-            inv *= d[i - 1];
-        }
-        f[1] = inv;
-        int const r0 = C.row0(jmin);
-#pragma unroll
-        for (int i = 0; i < D + 1; ++i) cc[i] = C.get(r0, i);
-        double y = 0.0;
-#pragma unroll
-        for (int r = 0; r < P + 1; ++r) {
-            double const den = kn[D + r] - kn[r];
-            y = fma(den != 0.0 ? (cc[r + 1] - cc[r]) * f[r + 1] : 0.0, v[r], y);
-        }
-        return y;
+        return nonuniform_deriv1<D>(eb, ck, x, C);
     }
     if (UNI) {
         double off;

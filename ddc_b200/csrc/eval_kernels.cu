@@ -6,8 +6,9 @@
 // gathering the degree+1 coefficients of each point from shared memory. The basis values are
 // computed in registers with the degree known at compile time. Derivatives of order n use the
 // derivative spline: n rounds of divided differences of the coefficients (de Boor, "A Practical
-// Guide to Splines", X.(15)) followed by the degree-(d-n) basis, which needs no division on device
-// (the knot-span inverses come from a table built with the evaluator).
+// Guide to Splines", X.(15)) followed by the degree-(d-n) basis. On non-uniform meshes, values and
+// first derivatives divide by knot differences (one batched division per level of the triangle);
+// higher orders read the knot-span inverses from a table built with the evaluator.
 #include <algorithm>
 
 #include "ddcb_internal.hpp"
@@ -43,7 +44,7 @@ __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src)
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
 }
 
-constexpr int kEvalThreads = 512;
+constexpr int kEvalThreads = 640; // 20 warps: one block per SM at up to 102 registers
 
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
 {
