@@ -154,9 +154,10 @@ __device__ __forceinline__ void nonuniform_values_span2(const double* kn, const 
 // Non-uniform Cox-de Boor values of degree P on the cell whose knots are kn (the layout of
 // nonuniform_values_span), dividing by the knot differences themselves: the j+1 denominators of
 // level j are inverted together with one division (prefix products, then one reciprocal, then
-// back-substitution of the products). Empty spans (repeated boundary knots) contribute 0. The
-// products hold at most P knot differences, so they stay in FP64 range for spacings between 1e-60
-// and 1e60 of the coordinate unit.
+// back-substitution of the products). Every denominator t[c+r+1] - t[c+r-j] spans the cell
+// [t_c, t_c+1), which is never empty (break points strictly increase), so no guard is needed even
+// where boundary knots repeat. The products hold at most P knot differences, so they stay in FP64
+// range for spacings between 1e-60 and 1e60 of the coordinate unit.
 template <int P>
 __device__ __forceinline__ void nonuniform_values_div(const double* kn, double x, double* v)
 {
@@ -170,7 +171,7 @@ __device__ __forceinline__ void nonuniform_values_div(const double* kn, double x
 #pragma unroll
         for (int r = 0; r <= j; ++r) {
             double const den = kn[P + r] - kn[P - 1 - j + r];
-            d[r] = den == 0.0 ? 1.0 : den;
+            d[r] = den;
             pre[r] = r == 0 ? d[0] : pre[r - 1] * d[r];
         }
         double inv = 1.0 / pre[j];
@@ -183,8 +184,7 @@ __device__ __forceinline__ void nonuniform_values_div(const double* kn, double x
         double saved = 0.0;
 #pragma unroll
         for (int r = 0; r < j + 1; ++r) {
-            double temp = v[r] * inv_d[r];
-            if (kn[P + r] == kn[P - 1 - j + r]) temp = 0.0;
+            double const temp = v[r] * inv_d[r];
             v[r] = saved + right[r] * temp;
             saved = left[j - r] * temp;
         }
@@ -194,7 +194,8 @@ __device__ __forceinline__ void nonuniform_values_div(const double* kn, double x
 
 // s'(x) on the non-uniform cell ck (spline_evaluator.hpp:357-478 for order 1): the 2D knots around
 // the cell give both the degree-(D-1) basis and the divided-difference factors
-// D / (t[jmin+i+D] - t[jmin+i]), computed here rather than read from the span table.
+// D / (t[ck+i] - t[ck-D+i]), i = 1..D, computed here rather than read from the span table. Each of
+// these spans contains the cell, so none is empty.
 template <int D, class Acc>
 __device__ __forceinline__ double nonuniform_deriv1(EvalBasis const& eb, int ck, double x, Acc const& C)
 {
@@ -208,7 +209,7 @@ __device__ __forceinline__ double nonuniform_deriv1(EvalBasis const& eb, int ck,
 #pragma unroll
     for (int i = 1; i <= D; ++i) {
         double const den = kn[D - 1 + i] - kn[i - 1];
-        d[i - 1] = den == 0.0 ? 1.0 : den;
+        d[i - 1] = den;
         pre[i - 1] = i == 1 ? d[0] : pre[i - 2] * d[i - 1];
     }
     double inv = double(D) / pre[D - 1];
@@ -224,9 +225,7 @@ __device__ __forceinline__ double nonuniform_deriv1(EvalBasis const& eb, int ck,
 #pragma unroll
     for (int r = 0; r < P + 1; ++r) {
         double const ci = C.get(r0, r + 1);
-        double a = (ci - cprev) * f[r + 1];
-        if (kn[D + r] == kn[r]) a = 0.0;
-        y = fma(a, v[r], y);
+        y = fma((ci - cprev) * f[r + 1], v[r], y);
         cprev = ci;
     }
     return y;
