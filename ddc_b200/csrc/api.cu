@@ -95,15 +95,24 @@ Evaluator* create_evaluator(Basis const& basis, int ex_lo, int ex_hi)
         std::vector<double> ispan(size_t(d) * nk, 0.0);
         for (int len = 1; len <= d; ++len)
             for (int i = 0; i + len < nk; ++i) ispan[size_t(len - 1) * nk + i] = inv(i, i + len);
-        // bucket table: the cell (knot index) holding the start of each of ncells uniform buckets
-        int const nb = std::max(1, D.ncells);
-        std::vector<int> lut(nb);
+        // bucket table over nb uniform buckets, at least one per cell and, up to 4 per cell and
+        // 4096 in all, no wider than the narrowest cell, so that a bucket holds at most one knot:
+        // {split, c0} with c0 the cell holding the bucket start and split the first knot inside
+        // the bucket (+inf if none)
+        int const last = d + D.ncells - 1;
+        double hmin = D.rmax - D.rmin;
+        for (int cc = d; cc <= last; ++cc) hmin = std::min(hmin, t[cc + 1] - t[cc]);
+        double const want = std::ceil((D.rmax - D.rmin) / hmin);
+        int const nb = std::max(std::max(1, D.ncells),
+                                int(std::min(want, double(std::min(4 * std::max(1, D.ncells), 4096)))));
+        std::vector<double> lut(size_t(2) * nb);
         double const scale = double(nb) / (D.rmax - D.rmin);
         int c = d;
         for (int bk = 0; bk < nb; ++bk) {
-            double const x0 = D.rmin + double(bk) / scale;
-            while (c < d + D.ncells - 1 && x0 >= t[c + 1]) ++c;
-            lut[bk] = c;
+            double const x0 = D.rmin + double(bk) / scale, x1 = D.rmin + double(bk + 1) / scale;
+            while (c < last && x0 >= t[c + 1]) ++c;
+            lut[2 * size_t(bk)] = (c < last && t[c + 1] < x1) ? t[c + 1] : HUGE_VAL;
+            lut[2 * size_t(bk) + 1] = double(c);
         }
         e->integrals.resize(e->basis.size());
         basis_integrals(e->basis, e->integrals.data());
@@ -112,7 +121,7 @@ Evaluator* create_evaluator(Basis const& basis, int ex_lo, int ex_hi)
         e->device = dev;
         upload_basis(e->basis, dev);
         auto up = [](size_t b) { return (b + 255) / 256 * 256; };
-        size_t const b_kp = kp.size() * 8, b_lut = lut.size() * 4, b_int = e->integrals.size() * 8;
+        size_t const b_kp = kp.size() * 8, b_lut = lut.size() * 8, b_int = e->integrals.size() * 8;
         size_t const b_isp = ispan.size() * 8;
         size_t const o_lut = up(b_kp), o_isp = o_lut + up(b_lut), o_int = o_isp + up(b_isp);
         size_t const total = o_int + b_int + 8;
@@ -125,7 +134,7 @@ Evaluator* create_evaluator(Basis const& basis, int ex_lo, int ex_hi)
         e->d_integrals = reinterpret_cast<double*>(base + o_int);
         e->eb.b = e->basis.device_desc();
         e->eb.kpairs = reinterpret_cast<double2 const*>(base);
-        e->eb.lut = reinterpret_cast<int const*>(base + o_lut);
+        e->eb.lut = reinterpret_cast<double2 const*>(base + o_lut);
         e->eb.inv_span = reinterpret_cast<double const*>(base + o_isp);
         e->eb.nbucket = nb;
         e->eb.bucket_scale = scale;

@@ -18,7 +18,9 @@ struct EvalBasis
     const double2* kpairs;    // nk-1 pairs (t_i, t_i+1): device copy, or shared-memory copy in a kernel
     const double* inv_span;   // degree x nk: inv_span[(len-1)*nk + i] = 1/(t[i+len] - t[i]) (0 if empty);
                               // global memory, or a shared-memory copy in a kernel (plain loads)
-    const int* lut;           // nbucket entries: knot index of the cell holding each bucket start
+    const double2* lut;       // nbucket entries {split, c0}: c0 the cell (knot index) holding the
+                              // bucket start, split the first knot inside the bucket (+inf if none);
+                              // device copy, or shared-memory copy in a kernel
     int nbucket;
     double bucket_scale;      // nbucket / (rmax - rmin)
     int nk;                   // number of knots
@@ -70,22 +72,49 @@ struct CoefGlobal
     __device__ __forceinline__ double get(int r0, int i) const { return __ldg(C + (int64_t)(r0 + i) * cs); }
 };
 
-// Cell of x as a knot index (the cell [t_c, t_c+1) with t_c <= x < t_c+1), with the end rules of
-// bsplines_non_uniform.hpp:666-695. A bucket table gives a starting cell; short walks finish it,
-// so the result equals the bisection's for any mesh.
-__device__ __forceinline__ int nonuniform_locate(EvalBasis const& eb, double x)
+// First guess of the cell of x as a knot index (the cell [t_c, t_c+1) with t_c <= x < t_c+1), with
+// the end rules of bsplines_non_uniform.hpp:666-695: the bucket's start cell, plus one past the
+// bucket's inner knot. Exact when the bucket holds at most one knot (the table is built with
+// buckets no wider than the narrowest cell, up to a size cap) and x is not within rounding of a
+// bucket edge; nonuniform_walk finishes it otherwise.
+__device__ __forceinline__ int nonuniform_guess(EvalBasis const& eb, double x)
 {
     int const d = eb.b.degree;
-    int const last = d + eb.b.ncells - 1;
     if (x <= eb.b.rmin) return d;
-    if (x >= eb.b.rmax) return last;
+    if (x >= eb.b.rmax) return d + eb.b.ncells - 1;
     int bk = static_cast<int>((x - eb.b.rmin) * eb.bucket_scale);
     bk = bk < 0 ? 0 : (bk >= eb.nbucket ? eb.nbucket - 1 : bk);
-    int c = __ldg(eb.lut + bk);
-    double2 p = eb.kpairs[c];
-    while (c < last && x >= p.y) p = eb.kpairs[++c];
-    while (c > d && x < p.x) p = eb.kpairs[--c];
+    double2 const e = eb.lut[bk];
+    return static_cast<int>(e.y) + (x >= e.x ? 1 : 0);
+}
+
+// Whether c is the cell of x, given tc = t_c and tc1 = t_c+1.
+__device__ __forceinline__ bool nonuniform_is_cell(EvalBasis const& eb, double x, int c, double tc, double tc1)
+{
+    int const d = eb.b.degree;
+    return (c == d || x >= tc) && (c == d + eb.b.ncells - 1 || x < tc1);
+}
+
+// The cell of x in [d, last], walking over the knot pairs from the guess c.
+__device__ __forceinline__ int nonuniform_walk_pairs(const double2* kpairs, int d, int last, double x, int c)
+{
+    double2 p = kpairs[c];
+    while (c < last && x >= p.y) p = kpairs[++c];
+    while (c > d && x < p.x) p = kpairs[--c];
     return c;
+}
+
+__device__ __forceinline__ int nonuniform_walk(EvalBasis const& eb, double x, int c)
+{
+    return nonuniform_walk_pairs(eb.kpairs, eb.b.degree, eb.b.degree + eb.b.ncells - 1, x, c);
+}
+
+// Cell of x: the guess, checked against its knot pair (equal to bisection for any mesh).
+__device__ __forceinline__ int nonuniform_locate(EvalBasis const& eb, double x)
+{
+    int const c = nonuniform_guess(eb, x);
+    double2 const p = eb.kpairs[c];
+    return nonuniform_is_cell(eb, x, c, p.x, p.y) ? c : nonuniform_walk(eb, x, c);
 }
 
 // The 2P knots t[c-P+1 .. c+P] around cell c (P >= 1), by P pair loads.
@@ -98,6 +127,20 @@ __device__ __forceinline__ void load_knots(EvalBasis const& eb, int c, double* k
         kn[2 * q] = p.x;
         kn[2 * q + 1] = p.y;
     }
+}
+
+// The cell of x and its 2P knots t[c-P+1 .. c+P] (P >= 1): the guess's knots hold t_c and t_c+1,
+// which check it; a wrong guess is walked to the cell and its knots reloaded.
+template <int P>
+__device__ __forceinline__ int locate_load_knots(EvalBasis const& eb, double x, double* kn)
+{
+    int c = nonuniform_guess(eb, x);
+    load_knots<P>(eb, c, kn);
+    if (!nonuniform_is_cell(eb, x, c, kn[P - 1], kn[P])) {
+        c = nonuniform_walk(eb, x, c);
+        load_knots<P>(eb, c, kn);
+    }
+    return c;
 }
 
 // Non-uniform Cox-de Boor values of degree P on cell c (bsplines_non_uniform.hpp:459-497), with
@@ -197,11 +240,11 @@ __device__ __forceinline__ void nonuniform_values_div(const double* kn, double x
 // D / (t[ck+i] - t[ck-D+i]), i = 1..D, computed here rather than read from the span table. Each of
 // these spans contains the cell, so none is empty.
 template <int D, class Acc>
-__device__ __forceinline__ double nonuniform_deriv1(EvalBasis const& eb, int ck, double x, Acc const& C)
+__device__ __forceinline__ double nonuniform_deriv1(EvalBasis const& eb, double x, Acc const& C)
 {
     constexpr int P = D - 1;
     double kn[2 * D]; // t[ck-D+1 .. ck+D]
-    load_knots<D>(eb, ck, kn);
+    int const ck = locate_load_knots<D>(eb, x, kn);
     double v[P + 1];
     if constexpr (P > 0) nonuniform_values_div<P>(kn + 1, x, v);
     else v[0] = 1.0;
@@ -242,10 +285,8 @@ __device__ __forceinline__ double eval_value_no_bc(EvalBasis const& eb, double x
         jmin = uniform_cell(eb.b, x, off);
         uniform_values_t<D>(off, v);
     } else {
-        int const ck = nonuniform_locate(eb, x);
-        jmin = ck - D;
         double kn[2 * D];
-        load_knots<D>(eb, ck, kn);
+        jmin = locate_load_knots<D>(eb, x, kn) - D;
         nonuniform_values_div<D>(kn, x, v);
     }
     int const r0 = C.row0(jmin);
@@ -286,8 +327,7 @@ __device__ __forceinline__ double eval_deriv_no_bc(EvalBasis const& eb, double x
     double v[P + 1];
     int jmin;
     if constexpr (!UNI && ORDER == 1) {
-        int const ck = nonuniform_locate(eb, x);
-        return nonuniform_deriv1<D>(eb, ck, x, C);
+        return nonuniform_deriv1<D>(eb, x, C);
     }
     if (UNI) {
         double off;

@@ -31,6 +31,7 @@ struct EvalArgs
     double* out;
     Lines lo;
     int pair16;         // coefs: adjacent line pairs 16-byte aligned and contiguous
+    int lut_smem;       // non-uniform: bucket table copied to shared memory after the knot pairs
 };
 
 __device__ __forceinline__ int64_t line_offset(Lines const& L, int64_t b)
@@ -80,13 +81,20 @@ __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const __grid_constan
         int64_t const oc = line_offset(a.lc, line);
         for (int r = c; r < a.size; r += nct) cp_async8(C + r * TLE + l, a.coefs + r * a.lc.stride + oc);
     }
-    if (!UNI)
+    double2* L = K + a.eb.nk; // bucket table (non-uniform, lut_smem)
+    if (!UNI) {
         for (int i = tid; i < a.eb.nk - 1; i += blockDim.x) cp_async16(K + i, a.eb.kpairs + i);
+        if (a.lut_smem)
+            for (int i = tid; i < a.eb.nbucket; i += blockDim.x) cp_async16(L + i, a.eb.lut + i);
+    }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
     if (!live) return;
     EvalBasis eb = a.eb;
-    if (!UNI) eb.kpairs = K;
+    if (!UNI) {
+        eb.kpairs = K;
+        if (a.lut_smem) eb.lut = L;
+    }
     int64_t const ox = line_offset(a.lx, line);
     int64_t const oo = line_offset(a.lo, line);
     int64_t const m = a.lx.n;
@@ -175,14 +183,24 @@ void launch_eval(Evaluator const& e, int order, double* out, Lines const& lo, do
     a.lo = lo;
     a.pair16 = line_pairs_aligned(coefs, lc);
     if (a.nlines == 0 || lx.n == 0) return;
-    // eight lines per block; two when the coefficient tile of eight long lines does not fit
-    auto bytes = [&](int tle) { return sizeof(double) * ((size_t)a.size * tle + (e.eb.b.uniform ? 0 : 2 * (size_t)e.eb.nk)); };
+    // eight lines per block, two when the coefficient tile of eight long lines does not fit; the
+    // bucket table of a non-uniform basis joins the knot pairs in shared memory when it fits too
+    bool const uni = e.eb.b.uniform != 0;
+    auto bytes = [&](int tle, bool lut) {
+        return sizeof(double) * ((size_t)a.size * tle + (uni ? 0 : 2 * ((size_t)e.eb.nk + (lut ? (size_t)e.eb.nbucket : 0))));
+    };
     int dev = 0, optin = 0;
     DDCB_CUDA_CHECK(cudaGetDevice(&dev));
     DDCB_CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    if (bytes(8) <= size_t(optin)) launch_deg<8>(a, order, bytes(8), s);
-    else if (bytes(2) <= size_t(optin)) launch_deg<2>(a, order, bytes(2), s);
-    else throw Error(DDCB_ERR_UNSUPPORTED, "a line of " + std::to_string(a.size) + " coefficients exceeds the evaluator's shared-memory tile");
+    for (int tle : {8, 2})
+        for (int lut = uni ? 0 : 1; lut >= 0; --lut)
+            if (bytes(tle, lut) <= size_t(optin)) {
+                a.lut_smem = lut;
+                if (tle == 8) launch_deg<8>(a, order, bytes(8, lut), s);
+                else launch_deg<2>(a, order, bytes(2, lut), s);
+                return;
+            }
+    throw Error(DDCB_ERR_UNSUPPORTED, "a line of " + std::to_string(a.size) + " coefficients exceeds the evaluator's shared-memory tile");
 }
 
 void launch_integrate(Evaluator const& e, double* out, int64_t out_outer_stride, double const* coefs, Lines const& lc,
