@@ -201,18 +201,21 @@ __device__ __forceinline__ void carry_scan(const R* __restrict__ Pm, typename Fa
         int const nb = FWD ? c - (1 << k) : c + (1 << k);
         bool const has = act && (FWD ? nb >= 0 : nb < NC);
         V v[K];
+        R mk[K * K];
         if (has) {
+            R const* M = Pm + ((size_t)k * NC + c) * K * K;
+#pragma unroll
+            for (int q = 0; q < K * K; ++q) mk[q] = __ldg(M + q);
 #pragma unroll
             for (int q = 0; q < K; ++q) v[q] = C2[(nb * KC + q) * P];
         }
         __syncthreads();
         if (has) {
-            R const* M = Pm + ((size_t)k * NC + c) * K * K;
 #pragma unroll
             for (int r = 0; r < K; ++r) {
                 V s = y[r];
 #pragma unroll
-                for (int q = 0; q < K; ++q) s = fma2(__ldg(M + r * K + q), v[q], s);
+                for (int q = 0; q < K; ++q) s = fma2(mk[r * K + q], v[q], s);
                 y[r] = s;
             }
 #pragma unroll
@@ -291,7 +294,7 @@ __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/,
             }
         }
         __syncthreads();
-        carry_scan<R, KL, KC, true>(Fac<R>::PhiF(t), carry, P, t.nscan, NC, c);
+        carry_scan<R, KL, KC, true>(Fac<R>::PhiF(t), carry, P, t.nscan_f, NC, c);
         if (c < NC) {
             V w[KL + 1];
 #pragma unroll
@@ -315,7 +318,7 @@ __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/,
             for (int q = 0; q < KU; ++q) carry[(c * KC + q) * P] = z[q];
         }
         __syncthreads();
-        carry_scan<R, KU, KC, false>(Fac<R>::PhiB(t), carry, P, t.nscan, NC, c);
+        carry_scan<R, KU, KC, false>(Fac<R>::PhiB(t), carry, P, t.nscan_b, NC, c);
         if (c < NC) {
             V z[KU];
 #pragma unroll

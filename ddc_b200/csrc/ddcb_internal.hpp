@@ -59,6 +59,8 @@ struct SolveTables
     int nchunk;      // chunks per line used by the sweeps
     int chunk_len;   // every chunk but the last has this (odd) length; the last absorbs the rest
     int nscan;       // steps of the log-depth carry scan: ceil(log2(nchunk))
+    int nscan_f, nscan_b; // steps the forward / backward scans run: the transfers of later steps
+                          // are below 2^-60 in every entry, so they change no carry
     int cj0, cj1, cshift; // rows [cj0, cj1) of Lf / piv / Uf are identical and stored once (at
                           // cj0); later rows move up by cshift = cj1 - cj0 - 1 (0: no run)
     const double* Lf;    // m x kl: Lf[j*kl + t-1] = multiplier of row j+t at step j

@@ -338,6 +338,7 @@ struct HostSolve
     bool pivot = false;
     // chunking
     long nchunk = 1, chunk_len = 0, nscan = 0;
+    long nscan_f = 0, nscan_b = 0; // scan steps run: later steps' transfers are below 2^-60
     std::vector<double> Lf, Uf, PhiF, PhiB;
     std::vector<int8_t> piv;
     long qg_lo = 0, qg_hi = 0;
@@ -607,6 +608,19 @@ struct HostSolve
                     matmul(&PhiB[((k - 1) * nchunk + c) * ku * ku], &PhiB[((k - 1) * nchunk + c + half) * ku * ku], Pb, ku);
             }
         }
+        // Step k of a scan adds P(k, c) times the true carry of chunk c -/+ 2^k; once every entry of
+        // every P(k, .) is below 2^-60, that term and those of all later steps (products with
+        // P(k, .) as a factor) are below FP64 rounding of the carries, so the scan stops there.
+        auto steps_needed = [&](std::vector<double> const& Pm, long K) {
+            for (long k = 0; k < nscan; ++k) {
+                double mx = 0.0;
+                for (long q = k * nchunk * K * K; q < (k + 1) * nchunk * K * K; ++q) mx = std::max(mx, std::fabs(Pm[q]));
+                if (mx <= 0x1p-60) return k;
+            }
+            return nscan;
+        };
+        nscan_f = kl > 0 ? steps_needed(PhiF, kl) : 0;
+        nscan_b = ku > 0 ? steps_needed(PhiB, ku) : 0;
     }
 
     // Full host solve of A x = rhs (or A^T x = rhs): used for quadrature coefficients.
@@ -712,6 +726,8 @@ SolveTables upload_tables(HostSolve const& h, std::vector<char>& blob, std::vect
     t.nchunk = int(h.nchunk);
     t.chunk_len = int(h.chunk_len);
     t.nscan = int(h.nscan);
+    t.nscan_f = int(h.nscan_f);
+    t.nscan_b = int(h.nscan_b);
     t.lam_nnz = int(h.lam_val.size());
     t.qg_lo = int(h.qg_lo);
     t.qg_hi = int(h.qg_hi);
@@ -1106,7 +1122,7 @@ static void emulate_tile_solve(HostSolve const& h, std::vector<double>& T)
     std::vector<double> carry(NC * std::max(KL, KU), 0.0), halo(NC * KL, 0.0);
     auto scan = [&](std::vector<double> const& P, long K, bool fwd) {
         std::vector<double> y(carry);
-        for (long s = 0; s < h.nscan; ++s) {
+        for (long s = 0; s < (fwd ? h.nscan_f : h.nscan_b); ++s) {
             std::vector<double> next(y);
             for (long c = 0; c < NC; ++c) {
                 long const nb = fwd ? c - (1L << s) : c + (1L << s);
