@@ -68,13 +68,6 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 
-// Row of the factor tables holding row j: runs of identical rows (the steady state of a
-// constant-coefficient band) are stored once (plan.cpp, upload_tables).
-__device__ __forceinline__ int crow(SolveTables const& t, int j)
-{
-    return j < t.cj0 ? j : (j < t.cj1 ? t.cj0 : j - t.cshift);
-}
-
 __device__ __forceinline__ double2 fma2(double a, double2 y, double2 w)
 {
     return make_double2(fma(a, y.x, w.x), fma(a, y.y, w.y));
@@ -118,18 +111,19 @@ struct Fac<float>
     __device__ static const float* Qg(SolveTables const& t) { return t.f32.Qg; }
 };
 
-// Forward sweep with L (and the row interchanges when PIV) over rows [a, e) of a line pair; T2
-// points at the pair's column (row j at T2[j*P]). w[0..KL-1] hold rows a..a+KL-1 on entry. Phase A
-// (WRITE false) reads rows beyond e from the tile, which nothing has written yet. Phase C (WRITE
-// true) writes rows a..e-1; without interchanges rows beyond e only feed the next chunk's rows,
-// so they are not read; with interchanges they come from the halo copy.
+// Forward sweep with L (and the row interchanges when PIV) over rows [a, e) (chunk c) of a line
+// pair; T2 points at the pair's column (row j at T2[j*P]). w[0..KL-1] hold rows a..a+KL-1 on
+// entry. Phase A (WRITE false) reads rows beyond e from the tile, which nothing has written yet.
+// Phase C (WRITE true) writes rows a..e-1; without interchanges rows beyond e only feed the next
+// chunk's rows, so they are not read; with interchanges they come from the halo copy.
 template <class R, int KL, bool PIV, bool WRITE, int UNR>
-__device__ __forceinline__ void fwd_sweep(SolveTables const& t, typename Fac<R>::V* T2, int P, int a, int e,
+__device__ __forceinline__ void fwd_sweep(SolveTables const& t, typename Fac<R>::V* T2, int P, int a, int e, int c,
                                           typename Fac<R>::V* w, const typename Fac<R>::V* halo, int hstride)
 {
     using V = typename Fac<R>::V;
     R const* __restrict__ Lf = Fac<R>::Lf(t);
     int const lim = (WRITE && !PIV) ? e : t.m; // fill rows below lim are read
+    int const qs = factor_stride(t);
 #pragma unroll UNR
     for (int j = a; j < e; ++j) {
         int const rr = j + KL;
@@ -137,9 +131,8 @@ __device__ __forceinline__ void fwd_sweep(SolveTables const& t, typename Fac<R>:
         if (rr < e) fill = T2[rr * P];
         else if (rr < lim) fill = (WRITE && PIV) ? halo[(rr - e) * hstride] : T2[rr * P];
         w[KL] = fill;
-        int const cj = crow(t, j);
         if (PIV) {
-            int const pv = __ldg(t.piv + cj);
+            int const pv = __ldg(t.piv + piv_index(t, j, a, c));
 #pragma unroll
             for (int q = 1; q <= KL; ++q)
                 if (pv == q) {
@@ -150,28 +143,29 @@ __device__ __forceinline__ void fwd_sweep(SolveTables const& t, typename Fac<R>:
         }
         V const y = w[0];
         if (WRITE) T2[j * P] = y;
-        R const* L = Lf + (size_t)cj * KL;
+        R const* L = Lf + factor_base(t, j, a, c, KL);
 #pragma unroll
-        for (int q = 1; q <= KL; ++q) w[q] = fma2(-__ldg(L + q - 1), y, w[q]);
+        for (int q = 1; q <= KL; ++q) w[q] = fma2(-__ldg(L + (q - 1) * qs), y, w[q]);
 #pragma unroll
         for (int q = 0; q < KL; ++q) w[q] = w[q + 1];
     }
 }
 
-// Backward sweep with U over rows e-1 .. a of a line pair; z[0..KU-1] hold the solution rows
-// e .. e+KU-1 (the carry from the chunk below) on entry.
+// Backward sweep with U over rows e-1 .. a (chunk c) of a line pair; z[0..KU-1] hold the solution
+// rows e .. e+KU-1 (the carry from the chunk below) on entry.
 template <class R, int KU, bool WRITE, int UNR>
-__device__ __forceinline__ void bwd_sweep(SolveTables const& t, typename Fac<R>::V* T2, int P, int a, int e,
+__device__ __forceinline__ void bwd_sweep(SolveTables const& t, typename Fac<R>::V* T2, int P, int a, int e, int c,
                                           typename Fac<R>::V* z)
 {
     using V = typename Fac<R>::V;
     R const* __restrict__ Uf = Fac<R>::Uf(t);
+    int const qs = factor_stride(t);
 #pragma unroll UNR
     for (int j = e - 1; j >= a; --j) {
-        R const* U = Uf + (size_t)crow(t, j) * (KU + 1);
+        R const* U = Uf + factor_base(t, j, a, c, KU + 1);
         V s = T2[j * P];
 #pragma unroll
-        for (int q = 1; q <= KU; ++q) s = fma2(-__ldg(U + q), z[q - 1], s);
+        for (int q = 1; q <= KU; ++q) s = fma2(-__ldg(U + q * qs), z[q - 1], s);
         V const x = mul2(s, __ldg(U));
         if (WRITE) T2[j * P] = x;
 #pragma unroll
@@ -284,8 +278,8 @@ __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/,
             V w[KL + 1];
 #pragma unroll
             for (int q = 0; q < KL; ++q) w[q] = (a + q < m) ? T2[(a + q) * P] : zero;
-            if (t.pivot) fwd_sweep<R, KL, true, false, UNR>(t, T2, P, a, e, w, nullptr, 0);
-            else fwd_sweep<R, KL, false, false, UNR>(t, T2, P, a, e, w, nullptr, 0);
+            if (t.pivot) fwd_sweep<R, KL, true, false, UNR>(t, T2, P, a, e, c, w, nullptr, 0);
+            else fwd_sweep<R, KL, false, false, UNR>(t, T2, P, a, e, c, w, nullptr, 0);
 #pragma unroll
             for (int q = 0; q < KL; ++q) {
                 V const orig = (e + q < m) ? T2[(e + q) * P] : zero;
@@ -303,8 +297,8 @@ __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/,
                 if (c > 0 && a + q < m) v = add2(v, carry[((c - 1) * KC + q) * P]);
                 w[q] = v;
             }
-            if (t.pivot) fwd_sweep<R, KL, true, true, UNR>(t, T2, P, a, e, w, halo + (size_t)c * KL * P, P);
-            else fwd_sweep<R, KL, false, true, UNR>(t, T2, P, a, e, w, nullptr, 0);
+            if (t.pivot) fwd_sweep<R, KL, true, true, UNR>(t, T2, P, a, e, c, w, halo + (size_t)c * KL * P, P);
+            else fwd_sweep<R, KL, false, true, UNR>(t, T2, P, a, e, c, w, nullptr, 0);
         }
         __syncthreads();
 
@@ -313,7 +307,7 @@ __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/,
             V z[KU];
 #pragma unroll
             for (int q = 0; q < KU; ++q) z[q] = zero;
-            bwd_sweep<R, KU, false, UNR>(t, T2, P, a, e, z);
+            bwd_sweep<R, KU, false, UNR>(t, T2, P, a, e, c, z);
 #pragma unroll
             for (int q = 0; q < KU; ++q) carry[(c * KC + q) * P] = z[q];
         }
@@ -323,7 +317,7 @@ __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/,
             V z[KU];
 #pragma unroll
             for (int q = 0; q < KU; ++q) z[q] = (c + 1 < NC) ? carry[((c + 1) * KC + q) * P] : zero;
-            bwd_sweep<R, KU, true, UNR>(t, T2, P, a, e, z);
+            bwd_sweep<R, KU, true, UNR>(t, T2, P, a, e, c, z);
         }
         __syncthreads();
     }

@@ -63,9 +63,10 @@ struct SolveTables
                           // are below 2^-60 in every entry, so they change no carry
     int cj0, cj1, cshift; // rows [cj0, cj1) of Lf / piv / Uf are identical and stored once (at
                           // cj0); later rows move up by cshift = cj1 - cj0 - 1 (0: no run)
-    const double* Lf;    // m x kl: Lf[j*kl + t-1] = multiplier of row j+t at step j
-    const int8_t* piv;   // m: pivot row offset at step j (ipiv[j] - j)
-    const double* Uf;    // m x (ku+1): [1/U_jj, U_j,j+1 .. U_j,j+ku]
+    int il;              // 1: Lf / piv / Uf interleaved by chunk (factor_base); 0: row-major, compressed
+    const double* Lf;    // per row j, kl entries: multiplier t-1 of row j+t at step j
+    const int8_t* piv;   // per row j: pivot row offset at step j (ipiv[j] - j)
+    const double* Uf;    // per row j, ku+1 entries: [1/U_jj, U_j,j+1 .. U_j,j+ku]
     const double* PhiF;  // nscan x nchunk x kl x kl: transfer over chunks c-2^k+1..c (forward)
     const double* PhiB;  // nscan x nchunk x ku x ku: transfer over chunks c..c+2^k-1 (backward)
     // border (k > 0)
@@ -86,6 +87,22 @@ struct SolveTables
     const int* a_col;
     const double* a_val;
 };
+
+// Where the factor entries of row j live in the uploaded tables. Row-major tables (il = 0) store a
+// row's `width` entries together, with the steady run [cj0, cj1) stored once. Interleaved tables
+// (il = 1, meshes without a steady run) store entry q of step s of every chunk side by side, at
+// (s * width + q) * nchunk + c, so the chunks a warp sweeps in step read one contiguous segment.
+// Row j is step j - a of the chunk c that starts at row a. Entry q is at base + q * factor_stride.
+DDCB_HD int factor_crow(SolveTables const& t, int j)
+{
+    return j < t.cj0 ? j : (j < t.cj1 ? t.cj0 : j - t.cshift);
+}
+DDCB_HD int factor_base(SolveTables const& t, int j, int a, int c, int width)
+{
+    return t.il ? ((j - a) * width) * t.nchunk + c : factor_crow(t, j) * width;
+}
+DDCB_HD int factor_stride(SolveTables const& t) { return t.il ? t.nchunk : 1; }
+DDCB_HD int piv_index(SolveTables const& t, int j, int a, int c) { return t.il ? (j - a) * t.nchunk + c : factor_crow(t, j); }
 
 // How the right-hand side rows are gathered from the inputs and how the coefficients are placed.
 struct RhsMap

@@ -759,13 +759,33 @@ SolveTables upload_tables(HostSolve const& h, std::vector<char>& blob, std::vect
     t.cj0 = int(best0);
     t.cj1 = int(best1);
     t.cshift = best1 > best0 ? int(best1 - best0 - 1) : 0;
+    // Without a steady run (non-uniform meshes) the chunks of a warp read different rows in every
+    // sweep step; interleaving the rows by chunk makes those reads one contiguous segment.
+    t.il = (best0 == m && h.nchunk > 1) ? 1 : 0;
     std::vector<double> Lc, Uc;
     std::vector<int8_t> pc;
-    for (long j = 0; j < m; ++j) {
-        if (j > best0 && j < best1) continue;
-        Lc.insert(Lc.end(), h.Lf.begin() + j * kl, h.Lf.begin() + (j + 1) * kl);
-        Uc.insert(Uc.end(), h.Uf.begin() + j * ku1, h.Uf.begin() + (j + 1) * ku1);
-        pc.push_back(h.piv[j]);
+    if (t.il) {
+        long const NC = h.nchunk;
+        long smax = 0;
+        for (long c = 0; c < NC; ++c) smax = std::max(smax, h.chunk_end(c) - h.chunk_begin(c));
+        Lc.assign(size_t(std::max<long>(smax * kl * NC, 1)), 0.0);
+        Uc.assign(size_t(std::max<long>(smax * ku1 * NC, 1)), 0.0);
+        pc.assign(size_t(std::max<long>(smax * NC, 1)), 0);
+        for (long c = 0; c < NC; ++c) {
+            long const a = h.chunk_begin(c), e = h.chunk_end(c);
+            for (long j = a; j < e; ++j) {
+                for (long q = 0; q < kl; ++q) Lc[size_t(factor_base(t, int(j), int(a), int(c), int(kl)) + q * NC)] = h.Lf[j * kl + q];
+                for (long q = 0; q < ku1; ++q) Uc[size_t(factor_base(t, int(j), int(a), int(c), int(ku1)) + q * NC)] = h.Uf[j * ku1 + q];
+                pc[size_t(piv_index(t, int(j), int(a), int(c)))] = h.piv[j];
+            }
+        }
+    } else {
+        for (long j = 0; j < m; ++j) {
+            if (j > best0 && j < best1) continue;
+            Lc.insert(Lc.end(), h.Lf.begin() + j * kl, h.Lf.begin() + (j + 1) * kl);
+            Uc.insert(Uc.end(), h.Uf.begin() + j * ku1, h.Uf.begin() + (j + 1) * ku1);
+            pc.push_back(h.piv[j]);
+        }
     }
     push(Lc.data(), Lc.size() * 8);
     push(pc.data(), pc.size());
@@ -1119,10 +1139,19 @@ double emulate_build(Builder const& b, double const* vals, double const* dlo, do
 static void emulate_tile_solve(HostSolve const& h, std::vector<double>& T)
 {
     long const m = h.m, k = h.k, KL = h.kl, KU = h.ku, NC = h.nchunk;
+    // the factor and transfer tables as the kernels receive them, read with the kernels' indexing
+    std::vector<char> blob;
+    std::vector<size_t> offs;
+    SolveTables tb = upload_tables(h, blob, offs);
+    bind_tables(tb, blob.data(), offs.data());
+    long const qs = factor_stride(tb);
+    auto Lf_at = [&](long j, long a, long c, long q) { return tb.Lf[factor_base(tb, int(j), int(a), int(c), int(KL)) + q * qs]; };
+    auto Uf_at = [&](long j, long a, long c, long q) { return tb.Uf[factor_base(tb, int(j), int(a), int(c), int(KU + 1)) + q * qs]; };
+    auto piv_at = [&](long j, long a, long c) { return long(tb.piv[piv_index(tb, int(j), int(a), int(c))]); };
     std::vector<double> carry(NC * std::max(KL, KU), 0.0), halo(NC * KL, 0.0);
-    auto scan = [&](std::vector<double> const& P, long K, bool fwd) {
+    auto scan = [&](double const* P, long K, bool fwd) {
         std::vector<double> y(carry);
-        for (long s = 0; s < (fwd ? h.nscan_f : h.nscan_b); ++s) {
+        for (long s = 0; s < (fwd ? tb.nscan_f : tb.nscan_b); ++s) {
             std::vector<double> next(y);
             for (long c = 0; c < NC; ++c) {
                 long const nb = fwd ? c - (1L << s) : c + (1L << s);
@@ -1147,10 +1176,10 @@ static void emulate_tile_solve(HostSolve const& h, std::vector<double>& T)
             for (long q = 0; q < KL; ++q) w[q] = (a + q < m) ? T[a + q] : 0.0;
             for (long j = a; j < e; ++j) {
                 w[KL] = (j + KL < m) ? T[j + KL] : 0.0;
-                long const p = h.piv[j];
+                long const p = piv_at(j, a, c);
                 if (p) std::swap(w[0], w[p]);
                 double const y = w[0];
-                for (long q = 1; q <= KL; ++q) w[q] -= h.Lf[j * KL + q - 1] * y;
+                for (long q = 1; q <= KL; ++q) w[q] -= Lf_at(j, a, c, q - 1) * y;
                 for (long q = 0; q < KL; ++q) w[q] = w[q + 1];
             }
             for (long q = 0; q < KL; ++q) {
@@ -1159,7 +1188,7 @@ static void emulate_tile_solve(HostSolve const& h, std::vector<double>& T)
                 halo[c * KL + q] = orig;
             }
         }
-        scan(h.PhiF, KL, true);
+        scan(tb.PhiF, KL, true);
         std::vector<double> Tn(T);
         for (long c = 0; c < NC; ++c) {
             long const a = h.chunk_begin(c), e = h.chunk_end(c);
@@ -1168,11 +1197,11 @@ static void emulate_tile_solve(HostSolve const& h, std::vector<double>& T)
             for (long j = a; j < e; ++j) {
                 long const rr = j + KL;
                 w[KL] = rr < e ? T[rr] : (rr < m ? halo[c * KL + rr - e] : 0.0);
-                long const p = h.piv[j];
+                long const p = piv_at(j, a, c);
                 if (p) std::swap(w[0], w[p]);
                 double const y = w[0];
                 Tn[j] = y;
-                for (long q = 1; q <= KL; ++q) w[q] -= h.Lf[j * KL + q - 1] * y;
+                for (long q = 1; q <= KL; ++q) w[q] -= Lf_at(j, a, c, q - 1) * y;
                 for (long q = 0; q < KL; ++q) w[q] = w[q + 1];
             }
         }
@@ -1184,22 +1213,22 @@ static void emulate_tile_solve(HostSolve const& h, std::vector<double>& T)
             std::vector<double> z(KU, 0.0);
             for (long j = e - 1; j >= a; --j) {
                 double s = T[j];
-                for (long q = 1; q <= KU; ++q) s -= h.Uf[j * (KU + 1) + q] * z[q - 1];
-                double const x = s * h.Uf[j * (KU + 1)];
+                for (long q = 1; q <= KU; ++q) s -= Uf_at(j, a, c, q) * z[q - 1];
+                double const x = s * Uf_at(j, a, c, 0);
                 for (long q = KU - 1; q >= 1; --q) z[q] = z[q - 1];
                 z[0] = x;
             }
             for (long q = 0; q < KU; ++q) carry[c * KU + q] = z[q];
         }
-        scan(h.PhiB, KU, false);
+        scan(tb.PhiB, KU, false);
         for (long c = 0; c < NC; ++c) {
             long const a = h.chunk_begin(c), e = h.chunk_end(c);
             std::vector<double> z(KU, 0.0);
             for (long q = 0; q < KU; ++q) z[q] = (c + 1 < NC) ? carry[(c + 1) * KU + q] : 0.0;
             for (long j = e - 1; j >= a; --j) {
                 double s = T[j];
-                for (long q = 1; q <= KU; ++q) s -= h.Uf[j * (KU + 1) + q] * z[q - 1];
-                double const x = s * h.Uf[j * (KU + 1)];
+                for (long q = 1; q <= KU; ++q) s -= Uf_at(j, a, c, q) * z[q - 1];
+                double const x = s * Uf_at(j, a, c, 0);
                 Tn[j] = x;
                 for (long q = KU - 1; q >= 1; --q) z[q] = z[q - 1];
                 z[0] = x;
