@@ -219,11 +219,12 @@ __device__ __forceinline__ void carry_scan(const R* __restrict__ Pm, typename Fa
     }
 }
 
-// Shared-memory doubles of one tile: the rows, the carries, the halo rows and the border scratch.
+// Shared-memory doubles of one tile: the rows, the carries, the halo rows (row interchanges only)
+// and the border scratch.
 __host__ __device__ inline size_t tile_doubles(SolveTables const& t, int TL, int KL, int KU)
 {
     int const KC = KL > KU ? KL : KU;
-    return (size_t)t.n * TL + (size_t)t.nchunk * KC * TL + (size_t)t.nchunk * KL * TL + (size_t)t.k * TL;
+    return (size_t)t.n * TL + (size_t)t.nchunk * KC * TL + (t.pivot ? (size_t)t.nchunk * KL * TL : 0) + (size_t)t.k * TL;
 }
 
 // Largest tile width in {TL, TL/2, ..., 2} whose shared memory (bytes(width)) fits in the
@@ -262,14 +263,14 @@ __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/,
     int const nthr = blockDim.x / P;                     // threads per pair
     V* const T2 = reinterpret_cast<V*>(smem) + p;        // n rows, stride P
     V* const carry = T2 + (size_t)n * P;                 // NC x KC rows
-    V* const halo = carry + (size_t)NC * KC * P;         // NC x KL rows
-    V* const btmp = halo + (size_t)NC * KL * P;          // k rows
+    V* const halo = carry + (size_t)NC * KC * P;         // NC x KL rows (row interchanges only)
+    V* const btmp = halo + (t.pivot ? (size_t)NC * KL * P : 0); // k rows
     V const zero = Fac<R>::zero();
 
     int a = 0, e = 0;
     if (c < NC) {
-        a = c * t.chunk_len;
-        e = (c == NC - 1) ? m : a + t.chunk_len;
+        a = c * t.chunk_len + 2 * max(0, c - t.chunk_split);
+        e = (c == NC - 1) ? m : a + t.chunk_len + (c >= t.chunk_split ? 2 : 0);
     }
 
     // ---- 2. forward sweep with L (and the row interchanges) ----

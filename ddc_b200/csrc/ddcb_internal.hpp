@@ -57,7 +57,8 @@ struct SolveTables
     int kl, ku;
     int pivot;       // 1 if any row interchange happened
     int nchunk;      // chunks per line used by the sweeps
-    int chunk_len;   // every chunk but the last has this (odd) length; the last absorbs the rest
+    int chunk_len;   // chunks [0, chunk_split) have this (odd) length, the later ones two rows
+    int chunk_split; // more; the last chunk ends at row m
     int nscan;       // steps of the log-depth carry scan: ceil(log2(nchunk))
     int nscan_f, nscan_b; // steps the forward / backward scans run: the transfers of later steps
                           // are below 2^-60 in every entry, so they change no carry

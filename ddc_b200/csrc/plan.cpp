@@ -337,7 +337,7 @@ struct HostSolve
     long kl = 0, ku = 0;       // effective L / U bandwidths
     bool pivot = false;
     // chunking
-    long nchunk = 1, chunk_len = 0, nscan = 0;
+    long nchunk = 1, chunk_len = 0, chunk_split = 1, nscan = 0;
     long nscan_f = 0, nscan_b = 0; // scan steps run: later steps' transfers are below 2^-60
     std::vector<double> Lf, Uf, PhiF, PhiB;
     std::vector<int8_t> piv;
@@ -346,8 +346,8 @@ struct HostSolve
     std::vector<int> lam_row, lam_col;
     std::vector<double> lam_val;
 
-    long chunk_begin(long c) const { return c * chunk_len; }
-    long chunk_end(long c) const { return (c == nchunk - 1) ? m : (c + 1) * chunk_len; }
+    long chunk_begin(long c) const { return c * chunk_len + 2 * std::max(0L, c - chunk_split); }
+    long chunk_end(long c) const { return (c == nchunk - 1) ? m : chunk_begin(c + 1); }
 
     // rows: the system in kernel order (the builder rotates the reference's boundary rows and
     // columns to the end); border: the number of trailing rows/cols solved through the Schur
@@ -546,17 +546,35 @@ struct HostSolve
             Uf[j * (ku + 1)] = 1.0 / lu.at(j, j);
             for (long t = 1; t <= ku; ++t) Uf[j * (ku + 1) + t] = (t <= lu.kl + lu.ku && j + t < m) ? lu.at(j, j + t) : 0.0;
         }
-        // chunking: odd chunk length (conflict-free shared-memory rows), at least max(kl,ku)+1 rows
+        // chunking: odd chunk lengths (conflict-free shared-memory rows), at least max(kl,ku)+1 rows.
+        // Chunks have length L or L+2, so the longest sweep (the critical path) is at most two rows
+        // above the average; when the remainder does not split that way the last chunk takes it.
         long const minlen = std::max<long>(std::max(kl, ku) + 1, 3);
         if (m == 0) {
             nchunk = 1;
             chunk_len = 0;
+            chunk_split = 1;
         } else {
             long L = (m + nchunk_req - 1) / std::max<long>(nchunk_req, 1);
             L = std::max(L, minlen);
             if (L % 2 == 0) L += 1;
             nchunk = std::max<long>(1, m / L);
-            if (nchunk == 1) L = m;
+            chunk_split = nchunk;
+            if (nchunk > 1) {
+                long nc = nchunk, r = m - nc * L;
+                if (r % 2) {
+                    --nc;
+                    r += L;
+                }
+                if (nc > 1 && r / 2 <= nc) {
+                    nchunk = nc;
+                    chunk_split = nc - r / 2;
+                }
+            }
+            if (nchunk == 1) {
+                L = m;
+                chunk_split = 1;
+            }
             chunk_len = L;
         }
         // transfer matrices of one chunk: Phi_c (forward, kl x kl), Psi_c (backward, ku x ku)
@@ -725,6 +743,7 @@ SolveTables upload_tables(HostSolve const& h, std::vector<char>& blob, std::vect
     t.pivot = h.pivot ? 1 : 0;
     t.nchunk = int(h.nchunk);
     t.chunk_len = int(h.chunk_len);
+    t.chunk_split = int(h.chunk_split);
     t.nscan = int(h.nscan);
     t.nscan_f = int(h.nscan_f);
     t.nscan_b = int(h.nscan_b);
