@@ -43,6 +43,7 @@ def parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--lines", type=int, default=1 << 16, help="batch lines per GPU")
     p.add_argument("--e2e-steps", type=int, default=0, help="steps of the host-buffer (e2e) timing; 0 = --steps")
+    p.add_argument("--e2e-slice", type=int, default=4096, help="lines per slice of the host pipeline (e2e)")
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU time of the baseline sample")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--tile-lines", type=int, default=0, help="builder tile width (0 = plan default)")
@@ -414,8 +415,13 @@ def run_ours(args):
     npts = pts.size
     total_pts = world * lines * (npts + m) / 2
     value = total_pts / (ms_step * 1e-3) / 1e9
-    # ---- end-to-end through the public API with host buffers ----
+    # ---- end-to-end through the public API with host buffers: the host pipeline
+    # (ddcb_host_pipeline_run) copies every step's inputs in and its result out, batch slices
+    # overlapping the kernels ----
     ke = args.e2e_steps or args.steps
+    pipe = D.HostPipeline(builder, ev, m, order=1, slice_lines=args.e2e_slice)
+    for _ in range(2):
+        pipe(h_vals, h_x, h_out, h_dlo, h_dhi, stream=s)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -423,12 +429,7 @@ def run_ours(args):
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(s)
     for _ in range(ke):
-        vals.copy_(h_vals, non_blocking=True)
-        dlo.copy_(h_dlo, non_blocking=True)
-        dhi.copy_(h_dhi, non_blocking=True)
-        x.copy_(h_x, non_blocking=True)
-        step_fused()
-        h_out.copy_(out, non_blocking=True)
+        pipe(h_vals, h_x, h_out, h_dlo, h_dhi, stream=s)
     e1.record(s)
     torch.cuda.synchronize()
     e_ms_total = e0.elapsed_time(e1)
@@ -437,6 +438,7 @@ def run_ours(args):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e_ms_total = float(tt.item())
     e2e_value = total_pts / (e_ms_total / ke * 1e-3) / 1e9
+    e2e_matches = bool(torch.equal(h_out, out.cpu()))  # the device-resident step ran on the same inputs
     h2d = sum(t.numel() * 8 for t in (h_vals, h_dlo, h_dhi, h_x))
     d2h = h_out.numel() * 8
     # ---- roofline of the dominant kernel: the fused build + derivative kernel when the step ran
@@ -489,7 +491,8 @@ def run_ours(args):
                                      "Gpts_per_s": total_pts / ((b_ms + e_ms) * 1e-3) / 1e9 / world}},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "steps": ke},
+                    "steps": ke, "path": f"ddcb_host_pipeline_run, {args.e2e_slice}-line slices, pinned host buffers",
+                    "matches_device_path": e2e_matches},
             "gpu_launches": args.steps if fused else 2 * args.steps,
             "clocks": clk,
         }

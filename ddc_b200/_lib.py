@@ -96,6 +96,9 @@ SIGNATURES = {
     "ddcb_batch_uneven_offsets": [_vp, _vp, _vp, _vp, _vp, _vp],
     "ddcb_batch_uneven_tune": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int32, _vp],
     "ddcb_batch_uneven_run": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "ddcb_host_pipeline_create": [_vp, _vp, C.c_int32, C.c_int64, C.c_int64, _pp],
+    "ddcb_host_pipeline_destroy": [_vp],
+    "ddcb_host_pipeline_run": [_vp, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp],
     "ddcb_build2d_workspace_bytes": [_vp, _vp, C.c_int64, C.POINTER(C.c_uint64)],
     "ddcb_build2d": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int64, _vp, C.c_uint64, _vp],
     "ddcb_eval2d": [_vp, _vp, C.c_int32, C.c_int32, _vp, _vp, _vp, C.c_int64, C.c_int64, _vp],

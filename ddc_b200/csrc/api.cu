@@ -698,6 +698,121 @@ ddcb_status ddcb_batch_uneven_run(ddcb_uneven_batch h, const double* vals, const
     });
 }
 
+struct ddcb_host_pipeline_t
+{
+    ddcb::HostPipeline* p = nullptr;
+};
+
+// A host layout the pipeline can cut along the batch: rows of the batch (outer == 1, rows apart by
+// at least a row), or one contiguous line per batch index (inner == 1, stride 1).
+static void check_host_layout(ddcb_lines const& l, char const* name)
+{
+    if (l.n == 0 || l.inner * l.outer == 0) return;
+    bool const rows = l.outer == 1 && l.stride >= l.inner;
+    bool const lines = l.inner == 1 && l.stride == 1 && l.outer_stride >= l.n;
+    if (!rows && !lines)
+        throw ddcb::Error(DDCB_ERR_UNSUPPORTED, std::string(name)
+                                                    + ": host layouts must hold the batch in rows (outer == 1) or one contiguous line "
+                                                      "per batch index (inner == 1, stride == 1)");
+}
+
+ddcb_status ddcb_host_pipeline_create(ddcb_builder hb, ddcb_evaluator he, int32_t order, int64_t npoints, int64_t slice_lines,
+                                      ddcb_host_pipeline* out)
+{
+    return guarded([&] {
+        require(hb && he && out, "NULL argument");
+        ddcb::Builder const& b = *hb->b;
+        ddcb::Evaluator const& e = *he->e;
+        require(order >= 0 && order <= e.basis.desc.degree, "derivative order must be in 0..degree");
+        require(e.basis.desc.degree == b.basis.desc.degree && e.basis.desc.ncells == b.basis.desc.ncells
+                    && e.basis.desc.uniform == b.basis.desc.uniform && e.basis.desc.periodic == b.basis.desc.periodic,
+                "builder and evaluator use different bases");
+        require(npoints >= 0, "negative number of evaluation points");
+        require(slice_lines >= 1 && slice_lines <= (int64_t(1) << 30), "slice_lines must be in 1..2^30");
+        int dev = 0;
+        DDCB_CUDA_CHECK(cudaGetDevice(&dev));
+        require(dev == b.device && dev == e.device, "the builder and the evaluator must live on the current device");
+        auto* h = new ddcb_host_pipeline_t();
+        try {
+            h->p = ddcb::create_host_pipeline(b, e, int(order), npoints, slice_lines);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+ddcb_status ddcb_host_pipeline_destroy(ddcb_host_pipeline h)
+{
+    return guarded([&] {
+        if (!h) return;
+        ddcb::destroy_host_pipeline(h->p);
+        delete h;
+    });
+}
+
+ddcb_status ddcb_host_pipeline_run(ddcb_host_pipeline h, const double* vals, ddcb_lines lv, const double* dlo, ddcb_lines llo,
+                                   const double* dhi, ddcb_lines lhi, const double* coords, ddcb_lines lx, double* out,
+                                   ddcb_lines lo, double* coefs, ddcb_lines lc, ddcb_stream stream)
+{
+    return guarded([&] {
+        require(h != nullptr, "pipeline is NULL");
+        ddcb::HostPipeline& p = *h->p;
+        ddcb::Builder const& b = *p.b;
+        int dev = 0;
+        DDCB_CUDA_CHECK(cudaGetDevice(&dev));
+        require(dev == p.device, "the pipeline was created for another device");
+        check_lines(lv, int64_t(b.points.size()), "vals");
+        check_lines(lx, p.m, "coords");
+        check_lines(lo, p.m, "out");
+        same_batch(lx, lv, "coords/vals");
+        same_batch(lo, lv, "out/vals");
+        check_host_layout(lv, "vals");
+        check_host_layout(lx, "coords");
+        check_host_layout(lo, "out");
+        if (coefs) {
+            check_lines(lc, b.basis.size(), "coefs");
+            same_batch(lc, lv, "coefs/vals");
+            check_host_layout(lc, "coefs");
+        }
+        if (b.lo == DDCB_HERMITE && b.nbv_lo > 0) {
+            require(dlo != nullptr, "derivs_lo is required by the lower HERMITE closure");
+            check_lines(llo, b.nbv_lo, "derivs_lo");
+            same_batch(llo, lv, "derivs_lo/vals");
+            check_host_layout(llo, "derivs_lo");
+        } else {
+            dlo = nullptr;
+        }
+        if (b.hi == DDCB_HERMITE && b.nbv_hi > 0) {
+            require(dhi != nullptr, "derivs_hi is required by the upper HERMITE closure");
+            check_lines(lhi, b.nbv_hi, "derivs_hi");
+            same_batch(lhi, lv, "derivs_hi/vals");
+            check_host_layout(lhi, "derivs_hi");
+        } else {
+            dhi = nullptr;
+        }
+        int64_t const nbatch = lv.inner * lv.outer;
+        if (nbatch == 0) return;
+        require(vals != nullptr, "vals pointer is NULL");
+        require(p.m == 0 || (coords && out), "coords/out pointer is NULL");
+        ddcb::HostArrays a;
+        a.vals = vals;
+        a.lv = ddcb::to_lines(lv);
+        a.dlo = dlo;
+        a.llo = ddcb::to_lines(llo);
+        a.dhi = dhi;
+        a.lhi = ddcb::to_lines(lhi);
+        a.coords = coords;
+        a.lx = ddcb::to_lines(lx);
+        a.out = out;
+        a.lo = ddcb::to_lines(lo);
+        a.coefs = coefs;
+        a.lc = ddcb::to_lines(lc);
+        ddcb::run_host_pipeline(p, nbatch, a, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
 ddcb_status ddcb_build2d_workspace_bytes(ddcb_builder b1, ddcb_builder b2, int64_t nbatch, uint64_t* bytes)
 {
     return guarded([&] {

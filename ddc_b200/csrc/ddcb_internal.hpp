@@ -217,6 +217,41 @@ bool launch_build_eval_adjoint(Builder const& b, Evaluator const& e, int order, 
                                Lines const& lgv, double* gdlo, Lines const& lglo, double* gdhi, Lines const& lghi,
                                double* gx, Lines const& lgx, cudaStream_t s);
 
+// host_pipeline.cu: build + evaluate on host buffers, batch slices pipelined over three streams.
+// Host layouts have outer == 1 (rows of the batch, any row stride >= inner) or inner == 1 with unit
+// stride (one contiguous line per batch index).
+struct HostArrays
+{
+    const double* vals = nullptr;
+    Lines lv {};
+    const double* dlo = nullptr; // NULL when the lower closure reads no derivative
+    Lines llo {};
+    const double* dhi = nullptr;
+    Lines lhi {};
+    const double* coords = nullptr;
+    Lines lx {};
+    double* out = nullptr;
+    Lines lo {};
+    double* coefs = nullptr; // optional copy of the coefficients
+    Lines lc {};
+};
+struct HostPipeline
+{
+    Builder const* b = nullptr;
+    Evaluator const* e = nullptr;
+    int order = 0;
+    int64_t m = 0;     // evaluation points per line
+    int64_t slice = 0; // lines per slice
+    int device = 0;
+    void* d_block = nullptr;
+    double* buf[2][6] = {}; // per buffer set: vals, derivs_lo, derivs_hi, coords, out, coefs
+    cudaStream_t s_in = nullptr, s_comp = nullptr, s_out = nullptr;
+    cudaEvent_t ev_start = nullptr, in_done[2] = {}, comp_done[2] = {}, out_done[2] = {};
+};
+HostPipeline* create_host_pipeline(Builder const& b, Evaluator const& e, int order, int64_t m, int64_t slice);
+void destroy_host_pipeline(HostPipeline* p);
+void run_host_pipeline(HostPipeline& p, int64_t nbatch, HostArrays const& h, cudaStream_t user);
+
 // uneven_batch.cu
 struct UnevenBatch;
 UnevenBatch* create_uneven_batch(Builder const* const* builders, Evaluator const* const* evals, int64_t const* nevals,

@@ -477,3 +477,56 @@ class UnevenBatch:
         _lib.call("ddcb_batch_uneven_run", self._h, *self._ptrs(vals, derivs_lo, derivs_hi, coefs, coords, out),
                   _stream_handle(stream))
         return out
+
+
+def _host_f64(t, name):
+    import torch
+
+    if t is None:
+        return None
+    if not (isinstance(t, torch.Tensor) and t.device.type == "cpu" and t.dtype == torch.float64):
+        raise TypeError(f"{name} must be a CPU float64 tensor (page-locked for asynchronous copies)")
+    return t
+
+
+class HostPipeline:
+    """SplineBuilder::operator() then SplineEvaluator (order 0) or ::deriv(order) on HOST tensors
+    (ddcb_host_pipeline_*): the batch runs in slices of `slice_lines` lines whose host-to-device
+    copies, kernels and device-to-host copies overlap on three streams. Host tensors use the layouts
+    of the device calls (interest dimension `dim`, batch in the other dimensions) with the batch
+    either in rows or one contiguous line per batch index; pin them (`pin_memory()`) for
+    asynchronous copies. The builder and evaluator are kept alive by the pipeline."""
+
+    def __init__(self, builder: SplineBuilder, evaluator: SplineEvaluator, npoints: int, *, order: int = 0,
+                 slice_lines: int = 8192):
+        self.builder, self.evaluator = builder, evaluator
+        h = C.c_void_p()
+        _lib.call("ddcb_host_pipeline_create", builder._h, evaluator._h, int(order), int(npoints), int(slice_lines),
+                  C.byref(h))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        L = getattr(_lib, "_lib", None) if _lib is not None else None
+        if h and L is not None:
+            L.ddcb_host_pipeline_destroy(h)
+            self._h = None
+
+    def __call__(self, vals, coords_eval, spline_eval, derivs_xmin=None, derivs_xmax=None, spline=None, *, dim: int = 0,
+                 stream=None):
+        """Reads vals / derivs / coords_eval and writes spline_eval (and spline, when given) on the
+        host; the work is queued on `stream` (default: the current CUDA stream): synchronize it
+        before reading the outputs."""
+        vals = _host_f64(vals, "vals")
+        x = _host_f64(coords_eval, "coords_eval")
+        out = _host_f64(spline_eval, "spline_eval")
+        dlo = _host_f64(derivs_xmin, "derivs_xmin")
+        dhi = _host_f64(derivs_xmax, "derivs_xmax")
+        coefs = _host_f64(spline, "spline")
+        empty = Lines(0, 1, 0, 0, 0)
+        _lib.call("ddcb_host_pipeline_run", self._h, _ptr(vals), lines_of(vals, dim), _ptr(dlo),
+                  lines_of(dlo, dim) if dlo is not None else empty, _ptr(dhi),
+                  lines_of(dhi, dim) if dhi is not None else empty, _ptr(x), lines_of(x, dim), _ptr(out),
+                  lines_of(out, dim), _ptr(coefs), lines_of(coefs, dim) if coefs is not None else empty,
+                  _stream_handle(stream))
+        return spline_eval

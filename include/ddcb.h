@@ -227,6 +227,29 @@ ddcb_status ddcb_batch_uneven_run(ddcb_uneven_batch b, const double* vals, const
                                   const double* derivs_hi, double* coefs, const double* coords, double* out,
                                   ddcb_stream stream);
 
+/* ---- host pipeline: ddcb_build_eval on HOST arrays. Where a DDC user copies host data to the
+ *      device (ddc::parallel_deepcopy), builds and evaluates (examples/characteristics_advection.cpp:
+ *      251-259) and copies the result back one step after the other, the pipeline cuts the batch
+ *      into slices of `slice_lines` lines and overlaps the copy-in of slice i+1 and the copy-out of
+ *      slice i-1 with the kernels of slice i (three streams, two device buffer sets, allocated at
+ *      creation). Host layouts are ddcb_lines with outer == 1 (rows of the batch, row stride >=
+ *      inner) or inner == 1 and stride == 1 (one contiguous line per batch index). Page-locked
+ *      host memory lets the copies run asynchronously. ------------------------------------------ */
+typedef struct ddcb_host_pipeline_t* ddcb_host_pipeline;
+/* order: 0 evaluates values (with the evaluator's boundary handling), k >= 1 the k-th derivative;
+ * npoints: evaluation points per line (coordinate layouts must have n == npoints). */
+ddcb_status ddcb_host_pipeline_create(ddcb_builder b, ddcb_evaluator e, int32_t order, int64_t npoints,
+                                      int64_t slice_lines, ddcb_host_pipeline* out);
+ddcb_status ddcb_host_pipeline_destroy(ddcb_host_pipeline p);
+/* Runs the step on host arrays; ordered after the work queued on `stream`, and `stream` waits
+ * for the last copy-out, so synchronizing it makes `out` (and `coefs`, which may be NULL) ready.
+ * derivs_lo / derivs_hi are read as in ddcb_build. */
+ddcb_status ddcb_host_pipeline_run(ddcb_host_pipeline p, const double* vals, ddcb_lines vals_layout,
+                                   const double* derivs_lo, ddcb_lines derivs_lo_layout, const double* derivs_hi,
+                                   ddcb_lines derivs_hi_layout, const double* coords, ddcb_lines coords_layout,
+                                   double* out, ddcb_lines out_layout, double* coefs, ddcb_lines coefs_layout,
+                                   ddcb_stream stream);
+
 /* ---- 2D tensor product: SplineBuilder2D / SplineEvaluator2D on two 1D plans, for the layout
  *      (x1, x2, batch) with the batch contiguous (the reference's layout_right of
  *      DiscreteDomain<X1, X2, batch...>). ----------------------------------------------------- */

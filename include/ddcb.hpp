@@ -182,4 +182,32 @@ private:
     Handle<ddcb_evaluator, ddcb_evaluator_destroy> m_h;
 };
 
+// The build + evaluate step on HOST arrays, batch slices of the copies overlapping the kernels
+// (ddcb_host_pipeline_*): what a DDC user writes around SplineBuilder and SplineEvaluator with
+// ddc::parallel_deepcopy, pipelined. order 0 evaluates values, k >= 1 the k-th derivative. The
+// builder and evaluator must outlive the pipeline.
+class HostPipeline
+{
+public:
+    HostPipeline(SplineBuilder const& b, SplineEvaluator const& e, int order, int64_t npoints, int64_t slice_lines = 4096)
+    {
+        ddcb_host_pipeline h = nullptr;
+        check(ddcb_host_pipeline_create(b.get(), e.get(), order, npoints, slice_lines, &h));
+        m_h = Handle<ddcb_host_pipeline, ddcb_host_pipeline_destroy>(h);
+    }
+    ddcb_host_pipeline get() const { return m_h.get(); }
+    // Queued on `stream`; synchronize it before reading out (and coefs, when given).
+    void operator()(double const* vals, ddcb_lines vals_layout, double const* coords, ddcb_lines coords_layout, double* out,
+                    ddcb_lines out_layout, double const* derivs_lo = nullptr, ddcb_lines derivs_lo_layout = {},
+                    double const* derivs_hi = nullptr, ddcb_lines derivs_hi_layout = {}, double* coefs = nullptr,
+                    ddcb_lines coefs_layout = {}, ddcb_stream stream = nullptr) const
+    {
+        check(ddcb_host_pipeline_run(get(), vals, vals_layout, derivs_lo, derivs_lo_layout, derivs_hi, derivs_hi_layout, coords,
+                                     coords_layout, out, out_layout, coefs, coefs_layout, stream));
+    }
+
+private:
+    Handle<ddcb_host_pipeline, ddcb_host_pipeline_destroy> m_h;
+};
+
 } // namespace ddcb

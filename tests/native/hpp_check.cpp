@@ -17,6 +17,8 @@ int main()
     auto moved = std::move(bs);
     try {
         ddcb::SplineBuilder b(moved, ddcb::SplineBuilderClosure::PERIODIC, ddcb::SplineBuilderClosure::PERIODIC);
+        ddcb::SplineEvaluator ev(moved);
+        ddcb::HostPipeline pipe(b, ev, 0, 16, 64);
         std::printf("OK builder created (a GPU is present): nbasis %lld\n", (long long)b.info().nbasis);
     } catch (std::runtime_error const& e) {
         std::printf("OK runtime_error: %s\n", e.what());
