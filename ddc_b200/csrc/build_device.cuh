@@ -195,11 +195,14 @@ __device__ __forceinline__ void carry_scan(const R* __restrict__ Pm, typename Fa
         int const nb = FWD ? c - (1 << k) : c + (1 << k);
         bool const has = act && (FWD ? nb >= 0 : nb < NC);
         V v[K];
-        R mk[K * K];
+        // the matrix is read before the barrier (its loads overlap the wait) when it is small
+        constexpr bool PRE = K <= 4;
+        R mk[PRE ? K * K : 1];
         if (has) {
-            R const* M = Pm + ((size_t)k * NC + c) * K * K;
+            if constexpr (PRE) {
 #pragma unroll
-            for (int q = 0; q < K * K; ++q) mk[q] = __ldg(M + q);
+                for (int q = 0; q < K * K; ++q) mk[q] = __ldg(Pm + (k * K * K + q) * NC + c);
+            }
 #pragma unroll
             for (int q = 0; q < K; ++q) v[q] = C2[(nb * KC + q) * P];
         }
@@ -209,7 +212,10 @@ __device__ __forceinline__ void carry_scan(const R* __restrict__ Pm, typename Fa
             for (int r = 0; r < K; ++r) {
                 V s = y[r];
 #pragma unroll
-                for (int q = 0; q < K; ++q) s = fma2(mk[r * K + q], v[q], s);
+                for (int q = 0; q < K; ++q) {
+                    R const mrq = PRE ? mk[PRE ? r * K + q : 0] : __ldg(Pm + (k * K * K + r * K + q) * NC + c);
+                    s = fma2(mrq, v[q], s);
+                }
                 y[r] = s;
             }
 #pragma unroll
@@ -246,15 +252,17 @@ inline int fit_tile_lines(int TL, Bytes bytes)
 // lines). The carries, halo and border scratch follow the n rows (tile_doubles elements of R in
 // all). On return (after a barrier) T holds the solution. Every thread of the block must call it;
 // TL is even and the block has at least nchunk * TL / 2 threads.
-template <int TL, int KL, int KU, class R = double>
+// UNR0 (0: the default) sets the rows unrolled per sweep step.
+template <int TL, int KL, int KU, class R = double, int UNR0 = 0>
 __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/, R* smem)
 {
     static_assert(TL % 2 == 0, "the solve works on line pairs");
     using V = typename Fac<R>::V;
     constexpr int P = TL / 2;
     constexpr int KC = KL > KU ? KL : KU;
-    constexpr int UNR = TL >= 4 ? 4 : 1; // rows unrolled per sweep step; a single line pair is not
-                                         // unrolled, which keeps its kernels free of spills
+    // rows unrolled per sweep step: 4 by default; a single line pair is not unrolled, which keeps
+    // its kernels free of spills
+    constexpr int UNR = UNR0 > 0 ? UNR0 : (TL >= 4 ? 4 : 1);
     int const n = t.n, m = t.m, k = t.k;
     int const NC = t.nchunk;
     int const tid = threadIdx.x;
@@ -432,11 +440,11 @@ __device__ __forceinline__ void gather_tile(BuildArgs const& args, double* T)
 
 // Steps 1-4 of a build. On return (after a barrier) T[j*TL + l] holds solution column j of line l,
 // for j < n.
-template <int TL, int KL, int KU>
+template <int TL, int KL, int KU, int UNR0 = 0>
 __device__ __forceinline__ void solve_tile(BuildArgs const& args, double* smem)
 {
     gather_tile<TL>(args, smem);
-    solve_in_tile<TL, KL, KU>(args.t, args.nct, smem);
+    solve_in_tile<TL, KL, KU, double, UNR0>(args.t, args.nct, smem);
 }
 
 // Tile row holding output row b: the solution of tile column j belongs to B-spline

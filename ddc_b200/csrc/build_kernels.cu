@@ -9,11 +9,14 @@ namespace ddcb {
 
 namespace {
 
-template <int TL, int KL, int KU>
-__global__ void __launch_bounds__(1024) build_kernel(const __grid_constant__ BuildArgs args)
+// MAXT: the largest block the instantiation takes. Blocks of up to 256 threads (64 chunks of
+// 8-line tiles, the default) get up to 128 registers, which lets the sweeps of narrow bands
+// unroll 8 rows and keep more factor loads in flight; larger blocks keep 64 registers.
+template <int TL, int KL, int KU, int MAXT>
+__global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 2 : 1) build_kernel(const __grid_constant__ BuildArgs args)
 {
     extern __shared__ __align__(16) double smem[];
-    solve_tile<TL, KL, KU>(args, smem);
+    solve_tile<TL, KL, KU, (MAXT <= 256 && TL >= 4 && KL + KU <= 6) ? 8 : 0>(args, smem);
     store_tile<TL>(args, smem);
 }
 
@@ -30,7 +33,7 @@ void launch_tl(BuildArgs const& args, cudaStream_t s)
     if (sm > size_t(optin))
         throw Error(DDCB_ERR_UNSUPPORTED, "line tile of " + std::to_string(sm) + " bytes exceeds shared memory (" + std::to_string(optin)
                                               + "); use fewer tile lines");
-    auto kern = build_kernel<TL, KL, KU>;
+    auto kern = TL * nct <= 256 ? build_kernel<TL, KL, KU, 256> : build_kernel<TL, KL, KU, 1024>;
     if (sm > 48 * 1024) DDCB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
     int64_t const grid = (args.nlines + TL - 1) / TL;
     kern<<<dim3((unsigned)grid), dim3(TL * nct), sm, s>>>(args);

@@ -68,8 +68,8 @@ struct SolveTables
     const double* Lf;    // per row j, kl entries: multiplier t-1 of row j+t at step j
     const int8_t* piv;   // per row j: pivot row offset at step j (ipiv[j] - j)
     const double* Uf;    // per row j, ku+1 entries: [1/U_jj, U_j,j+1 .. U_j,j+ku]
-    const double* PhiF;  // nscan x nchunk x kl x kl: transfer over chunks c-2^k+1..c (forward)
-    const double* PhiB;  // nscan x nchunk x ku x ku: transfer over chunks c..c+2^k-1 (backward)
+    const double* PhiF;  // transfer over chunks c-2^k+1..c (forward), kl x kl, at scan_index
+    const double* PhiB;  // transfer over chunks c..c+2^k-1 (backward), ku x ku, at scan_index
     // border (k > 0)
     int lam_nnz;
     const int* lam_row;   // k+1 row pointers into lam_col / lam_val
@@ -104,6 +104,8 @@ DDCB_HD int factor_base(SolveTables const& t, int j, int a, int c, int width)
 }
 DDCB_HD int factor_stride(SolveTables const& t) { return t.il ? t.nchunk : 1; }
 DDCB_HD int piv_index(SolveTables const& t, int j, int a, int c) { return t.il ? (j - a) * t.nchunk + c : factor_crow(t, j); }
+// Entry e (row-major in the K x K matrix) of the transfer product of scan step k and chunk c.
+DDCB_HD int scan_index(SolveTables const& t, int k, int e, int c, int K) { return (k * K * K + e) * t.nchunk + c; }
 
 // How the right-hand side rows are gathered from the inputs and how the coefficients are placed.
 struct RhsMap

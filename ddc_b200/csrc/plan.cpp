@@ -806,11 +806,22 @@ SolveTables upload_tables(HostSolve const& h, std::vector<char>& blob, std::vect
             pc.push_back(h.piv[j]);
         }
     }
+    // transfer products entry-major, [k][entry][chunk] (scan_index), so the chunks a warp scans
+    // read one contiguous segment per entry
+    auto entry_major = [&](std::vector<double> const& P, long K) {
+        std::vector<double> o(P.size(), 0.0);
+        long const NC = h.nchunk;
+        for (long k = 0; k < h.nscan; ++k)
+            for (long c = 0; c < NC; ++c)
+                for (long e = 0; e < K * K; ++e) o[size_t(scan_index(t, int(k), int(e), int(c), int(K)))] = P[size_t((k * NC + c) * K * K + e)];
+        return o;
+    };
+    std::vector<double> const PhiFc = entry_major(h.PhiF, kl), PhiBc = entry_major(h.PhiB, h.ku);
     push(Lc.data(), Lc.size() * 8);
     push(pc.data(), pc.size());
     push(Uc.data(), Uc.size() * 8);
-    push(h.PhiF.data(), h.PhiF.size() * 8);
-    push(h.PhiB.data(), h.PhiB.size() * 8);
+    push(PhiFc.data(), PhiFc.size() * 8);
+    push(PhiBc.data(), PhiBc.size() * 8);
     push(h.lam_row.data(), h.lam_row.size() * 4);
     push(h.lam_col.data(), h.lam_col.size() * 4);
     push(h.lam_val.data(), h.lam_val.size() * 8);
@@ -823,8 +834,8 @@ SolveTables upload_tables(HostSolve const& h, std::vector<char>& blob, std::vect
     };
     push32(Lc);
     push32(Uc);
-    push32(h.PhiF);
-    push32(h.PhiB);
+    push32(PhiFc);
+    push32(PhiBc);
     push32(h.lam_val);
     push32(h.Sinv);
     push32(h.qg_rows);
@@ -872,7 +883,8 @@ std::string describe(HostSolve const& h)
 {
     return "border=" + std::to_string(h.k) + ",Q=BandLU(" + std::to_string(h.m) + ",kl=" + std::to_string(h.kl)
            + ",ku=" + std::to_string(h.ku) + (h.pivot ? ",pivoting" : "") + "),chunks=" + std::to_string(h.nchunk)
-           + "x" + std::to_string(h.chunk_len);
+           + "x" + std::to_string(h.chunk_len) + ",scan=" + std::to_string(h.nscan_f) + "/" + std::to_string(h.nscan_b) + "of"
+           + std::to_string(h.nscan);
 }
 
 } // namespace
@@ -1175,10 +1187,9 @@ static void emulate_tile_solve(HostSolve const& h, std::vector<double>& T)
             for (long c = 0; c < NC; ++c) {
                 long const nb = fwd ? c - (1L << s) : c + (1L << s);
                 if (nb < 0 || nb >= NC) continue;
-                double const* M = &P[(s * NC + c) * K * K];
                 for (long r = 0; r < K; ++r) {
                     double acc = y[c * K + r];
-                    for (long q = 0; q < K; ++q) acc += M[r * K + q] * y[nb * K + q];
+                    for (long q = 0; q < K; ++q) acc += P[scan_index(tb, int(s), int(r * K + q), int(c), int(K))] * y[nb * K + q];
                     next[c * K + r] = acc;
                 }
             }
