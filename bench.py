@@ -162,6 +162,15 @@ def cpu_reference_rate(lines_sample, seconds, threads=None):
     return pts_per_rep * reps / t_total / 1e9, nt, reps, t_total
 
 
+def workload_config(lines, m, world):
+    """The `config` of both arms' JSON lines: the workload the metric is quoted on."""
+    return {"workload": "non-uniform quintic Hermite B-splines, 1024 cells (1025 points + 2x2 derivatives), "
+                        f"{lines} lines per GPU in (x, batch) layout, build + first derivative at {m} random points "
+                        "per line",
+            "lines_per_gpu": lines, "degree": 5, "ncells": 1024, "eval_points_per_line": m,
+            "l2": "inputs larger than L2 (2.2 GB touched per step)", "parallelism": f"batch-sharded x{world}"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -181,8 +190,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "non-uniform quintic Hermite, 1024 cells, 65536 lines, build + d/dx at 1024 pts/line",
-                   "sample_lines_per_step": sample},
+        "config": {**workload_config(args.lines, 1024, args.gpus), "sample_lines_per_step": sample},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nt, "kind": "port",
                          "sample": f"{sample} lines per step (build + first-derivative eval), oracle/ restatement "
                                    "of the reference's LAPACK path with its thread-per-line OpenMP schedule"},
@@ -476,13 +484,8 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "non-uniform quintic Hermite B-splines, 1024 cells (1025 points + 2x2 derivatives), "
-                                   "65536 lines per GPU in (x, batch) layout, build + first derivative at 1024 random "
-                                   "points per line",
-                       "lines_per_gpu": lines, "degree": 5, "ncells": 1024, "eval_points_per_line": m,
-                       "l2": "inputs larger than L2 (2.2 GB touched per step)",
-                       "schedule": "fused build+deriv kernel" if fused else "builder kernel then evaluator kernel",
-                       "parallelism": f"batch-sharded x{world}"},
+            "config": {**workload_config(lines, m, world),
+                       "schedule": "fused build+deriv kernel" if fused else "builder kernel then evaluator kernel"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "kernel": kname,
                          "algorithmic_bytes_per_launch": kbytes, "peak_kind": peak_kind},
