@@ -183,8 +183,10 @@ void launch_eval(Evaluator const& e, int order, double* out, Lines const& lo, do
     a.lo = lo;
     a.pair16 = line_pairs_aligned(coefs, lc);
     if (a.nlines == 0 || lx.n == 0) return;
-    // eight lines per block, two when the coefficient tile of eight long lines does not fit; the
-    // bucket table of a non-uniform basis joins the knot pairs in shared memory when it fits too
+    // sixteen lines per block (a warp then reads two whole 128-byte tile rows per coefficient, and
+    // the tile fills move 128-byte row segments), eight or two when the coefficient tile of long
+    // lines does not fit; the bucket table of a non-uniform basis joins the knot pairs in shared
+    // memory when it fits too
     bool const uni = e.eb.b.uniform != 0;
     auto bytes = [&](int tle, bool lut) {
         return sizeof(double) * ((size_t)a.size * tle + (uni ? 0 : 2 * ((size_t)e.eb.nk + (lut ? (size_t)e.eb.nbucket : 0))));
@@ -192,11 +194,12 @@ void launch_eval(Evaluator const& e, int order, double* out, Lines const& lo, do
     int dev = 0, optin = 0;
     DDCB_CUDA_CHECK(cudaGetDevice(&dev));
     DDCB_CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    for (int tle : {8, 2})
+    for (int tle : {16, 8, 2})
         for (int lut = uni ? 0 : 1; lut >= 0; --lut)
             if (bytes(tle, lut) <= size_t(optin)) {
                 a.lut_smem = lut;
-                if (tle == 8) launch_deg<8>(a, order, bytes(8, lut), s);
+                if (tle == 16) launch_deg<16>(a, order, bytes(16, lut), s);
+                else if (tle == 8) launch_deg<8>(a, order, bytes(8, lut), s);
                 else launch_deg<2>(a, order, bytes(2, lut), s);
                 return;
             }
