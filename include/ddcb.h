@@ -243,7 +243,9 @@ ddcb_status ddcb_host_pipeline_create(ddcb_builder b, ddcb_evaluator e, int32_t 
 ddcb_status ddcb_host_pipeline_destroy(ddcb_host_pipeline p);
 /* Runs the step on host arrays; ordered after the work queued on `stream`, and `stream` waits
  * for the last copy-out, so synchronizing it makes `out` (and `coefs`, which may be NULL) ready.
- * derivs_lo / derivs_hi are read as in ddcb_build. */
+ * derivs_lo / derivs_hi are read as in ddcb_build. Successive runs of one pipeline are ordered on
+ * the device by its own events; calls from several host threads on one pipeline must not overlap
+ * in time (use one pipeline per thread). */
 ddcb_status ddcb_host_pipeline_run(ddcb_host_pipeline p, const double* vals, ddcb_lines vals_layout,
                                    const double* derivs_lo, ddcb_lines derivs_lo_layout, const double* derivs_hi,
                                    ddcb_lines derivs_hi_layout, const double* coords, ddcb_lines coords_layout,
