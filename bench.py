@@ -11,8 +11,11 @@ metric: Gpts/s = (lines * interpolation points + lines * evaluation points) / 2 
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-N > 1 runs under torchrun, one rank per GPU, every rank processing its own 65536 lines (weak
-scaling, no collective on the data path); time = max over ranks of the CUDA-event time.
+N > 1 runs one rank per GPU (the script starts torchrun itself when it is not already under it):
+the global batch is N x 65536 lines and every rank builds and evaluates its own contiguous shard of
+it (weak scaling, no collective on the data path); time = max over ranks of the CUDA-event time.
+`--cpu-stub` runs the same rank logic (launch, sharding, timing, max over ranks) on CPU ranks over
+gloo with a small NumPy step in place of the GPU kernels, for testing the multi-rank plumbing.
 `--impl reference` times the reference algorithm's CPU restatement (oracle/, the reference's
 schedule: host factorisation, thread-per-line sweeps, OpenMP over lines) on a bounded sample.
 """
@@ -49,6 +52,8 @@ def parse():
     p.add_argument("--tile-lines", type=int, default=0, help="builder tile width (0 = plan default)")
     p.add_argument("--chunks", type=int, default=0, help="builder chunks per line (0 = plan default)")
     p.add_argument("--no-configs", action="store_true", help="skip the other configurations' measurements")
+    p.add_argument("--cpu-stub", action="store_true",
+                   help="CPU ranks (gloo) with a NumPy step in place of the GPU kernels: checks the rank logic only")
     p.add_argument("--profile-case", choices=["adjoint", "periodic_cubic", "tensor2d"], default=None,
                    help="run only this case's kernels, --steps times on --lines lines (for profilers; prints no JSON line)")
     return p.parse_args()
@@ -124,11 +129,106 @@ def workload_plan(D, lines):
     return bs, pts, br
 
 
-def make_inputs(pts, lines, m, seed_offset=0):
+def make_inputs(pts, lines, m, line0=0, total=None):
+    """Inputs of lines [line0, line0 + lines) of a batch of `total` lines."""
     from ddc_b200 import workloads
 
-    w = workloads.config2(B=lines, points=pts, m=m)
-    return w
+    return workloads.config2(B=lines, points=pts, m=m, line0=line0, total=total)
+
+
+class Ranks:
+    """One process per GPU (or per CPU rank under --cpu-stub): rank / world from the torchrun
+    environment, the process group, this rank's shard of the global batch and the max over ranks."""
+
+    def __init__(self, backend, device=None):
+        import torch.distributed as dist
+
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.dist = dist if self.world > 1 else None
+        if self.dist is not None:
+            from datetime import timedelta
+
+            kw = {"device_id": device} if device is not None else {}
+            dist.init_process_group(backend, timeout=timedelta(seconds=120), **kw)
+
+    def shard(self, lines_per_rank):
+        """[start, stop) of this rank's lines in the global batch of world * lines_per_rank lines."""
+        from ddc_b200.sharding import shard_range
+
+        return shard_range(self.world * lines_per_rank, self.rank, self.world)
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max(self, value, device=None):
+        """Max of a float over ranks (every rank takes part)."""
+        if self.dist is None:
+            return float(value)
+        import torch
+
+        t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def gather(self, obj):
+        if self.dist is None:
+            return [obj]
+        out = [None] * self.world
+        self.dist.all_gather_object(out, obj)
+        return out
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+
+
+def run_cpu_stub(args):
+    """The multi-rank logic of run_ours on CPU ranks (gloo): each rank draws its shard of the global
+    batch, times a NumPy stand-in for the kernels (the sum of its samples times its coordinates)
+    over `steps` steps after `warmup`, and rank 0 prints the JSON line with the max over ranks.
+    Only the plumbing is under test here; no number it prints is a measurement of the path."""
+    R = Ranks("gloo")
+    lines, m = args.lines, 64
+    start, stop = R.shard(lines)
+    pts = np.linspace(0.0, 1.0, 33)
+    w = make_inputs(pts, stop - start, m, line0=start, total=R.world * lines)
+    step = lambda: float(w["vals"].sum() + w["coords"].sum())
+    for _ in range(args.warmup):
+        step()
+    R.barrier()
+    t0 = time.perf_counter()
+    check = 0.0
+    for _ in range(args.steps):
+        check = step()
+    ms = (time.perf_counter() - t0) * 1e3
+    ms_max = R.max(ms)
+    shards = R.gather([start, stop, check])
+    if R.rank == 0:
+        total = R.world * lines * (pts.size + m) / 2
+        print(json.dumps({"impl": "cpu-stub", "metric": METRIC, "value": total / (ms_max / args.steps * 1e-3) / 1e9,
+                          "unit": UNIT, "n_gpus": R.world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": ms_max / args.steps, "scaling": "weak",
+                          "config": {"lines_per_gpu": lines, "global_lines": R.world * lines,
+                                     "parallelism": f"batch-sharded x{R.world}"},
+                          "shards": shards}), flush=True)
+    R.close()
+
+
+def relaunch_under_torchrun(args):
+    """--gpus N > 1 outside torchrun: start N ranks (this script under torchrun, 127.0.0.1) and
+    return their exit status; rank 0 prints the JSON line."""
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.call(cmd)
 
 
 def algorithmic_bytes(lines, npts, nder, ncoef, m):
@@ -341,25 +441,24 @@ def measure_configs(peak, reps):
 
 def run_ours(args):
     import torch
-    import torch.distributed as dist
 
     import ddc_b200 as D
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available() or local >= torch.cuda.device_count():
+        raise RuntimeError(f"rank {local} has no CUDA device (found {torch.cuda.device_count()})")
     torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
-    lines, m = args.lines, 1024
+    dev = torch.device("cuda", local)
+    R = Ranks("nccl", dev)
+    world, rank = R.world, R.rank
+    # this rank's shard of the global batch (world x --lines lines); no collective on the data path
+    start, stop = R.shard(args.lines)
+    lines, m = stop - start, 1024
     bs, pts, br = workload_plan(D, lines)
     builder = D.SplineBuilder(bs, pts, D.SplineBuilderClosure.HERMITE, D.SplineBuilderClosure.HERMITE,
                               tile_lines=args.tile_lines, chunks=args.chunks)
     ev = D.SplineEvaluator(bs)
-    w = make_inputs(pts, lines, m)
-    dev = torch.device("cuda", local)
+    w = make_inputs(pts, lines, m, line0=start, total=world * args.lines)
     h_vals = torch.from_numpy(w["vals"]).pin_memory()
     h_dlo = torch.from_numpy(w["dlo"]).pin_memory()
     h_dhi = torch.from_numpy(w["dhi"]).pin_memory()
@@ -381,16 +480,14 @@ def run_ours(args):
         step_fused()
         step_two_calls()
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    R.barrier()
     fused = builder.build_and_evaluate(ev, coefs, vals, x, out, dlo, dhi, order=1)
     # ---- device-resident timing of the fused step (inputs > L2: 2.2 GB touched per step) ----
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    R.barrier()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
@@ -417,10 +514,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     b_ms = float(np.mean([a.elapsed_time(b) for a, b in ev_b]))
     e_ms = float(np.mean([a.elapsed_time(b) for a, b in ev_e]))
-    if world > 1:
-        tt = torch.tensor([ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = R.max(ms, dev)
     ms_step = ms / args.steps
     npts = pts.size
     total_pts = world * lines * (npts + m) / 2
@@ -433,8 +527,7 @@ def run_ours(args):
     for _ in range(2):
         pipe(h_vals, h_x, h_out, h_dlo, h_dhi, stream=s)
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    R.barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(s)
@@ -443,10 +536,7 @@ def run_ours(args):
     e1.record(s)
     torch.cuda.synchronize()
     e_ms_total = e0.elapsed_time(e1)
-    if world > 1:
-        tt = torch.tensor([e_ms_total], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e_ms_total = float(tt.item())
+    e_ms_total = R.max(e_ms_total, dev)
     e2e_value = total_pts / (e_ms_total / ke * 1e-3) / 1e9
     e2e_matches = bool(torch.equal(h_out, out.cpu()))  # the device-resident step ran on the same inputs
     h2d = sum(t.numel() * 8 for t in (h_vals, h_dlo, h_dhi, h_x))
@@ -507,9 +597,7 @@ def run_ours(args):
             except Exception as exc:  # reported, not required for the headline line
                 result["configs"] = {"error": f"{type(exc).__name__}: {exc}"}
         print(json.dumps(result), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    R.close()
     return result
 
 
@@ -557,6 +645,11 @@ def profile_case(args):
 
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(relaunch_under_torchrun(args))
+    if args.cpu_stub:
+        run_cpu_stub(args)
+        return
     if args.profile_case:
         profile_case(args)
         return

@@ -13,9 +13,16 @@ _GOLDEN = np.uint64(0x9E3779B97F4A7C15)
 
 def splitmix_uniform(seed: int, stream: int, n: int) -> np.ndarray:
     """n uniforms in [0, 1) from the splitmix64 sequence of (seed, stream)."""
+    return splitmix_at(seed, stream, np.arange(n, dtype=np.uint64))
+
+
+def splitmix_at(seed: int, stream: int, idx) -> np.ndarray:
+    """Uniforms number idx (0-based, any shape) of the splitmix64 sequence of (seed, stream): a shard
+    of a batch draws exactly the numbers the whole batch would give its lines."""
+    idx = np.asarray(idx, dtype=np.uint64)
     with np.errstate(over="ignore"):
         base = np.uint64((seed + (stream << 40)) & 0xFFFFFFFFFFFFFFFF)
-        x = base + (np.arange(1, n + 1, dtype=np.uint64) * _GOLDEN)
+        x = base + ((idx + np.uint64(1)) * _GOLDEN)
         z = x
         z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
         z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
@@ -53,18 +60,25 @@ def config2_breaks(ncells: int = 1024):
     return br
 
 
-def config2(B: int = 1 << 16, ncells: int = 1024, m: int = 1024, points=None):
-    """Non-uniform quintic, Hermite closures (derivative orders 1 and 2 per side), d/dx evaluation."""
+def config2(B: int = 1 << 16, ncells: int = 1024, m: int = 1024, points=None, line0: int = 0, total=None):
+    """Non-uniform quintic, Hermite closures (derivative orders 1 and 2 per side), d/dx evaluation.
+    Lines [line0, line0 + B) of a batch of `total` lines (default B): a rank's shard of a larger
+    batch holds the same inputs as those lines of the whole batch."""
     seed = 0xDDC0 + 2
+    total = B if total is None else total
+    if not 0 <= line0 and line0 + B <= total:
+        raise ValueError("the lines must lie inside the batch")
     br = config2_breaks(ncells)
-    k = np.floor(splitmix_uniform(seed, 2, B) * 8).astype(np.int64) + 1
-    ph = splitmix_uniform(seed, 3, B) * 2 * np.pi
+    lines = np.arange(line0, line0 + B, dtype=np.uint64)
+    k = np.floor(splitmix_at(seed, 2, lines) * 8).astype(np.int64) + 1
+    ph = splitmix_at(seed, 3, lines) * 2 * np.pi
     out = dict(degree=5, ncells=ncells, breaks=br, k=k, ph=ph)
     if points is not None:
         out["vals"] = np.ascontiguousarray(cos_family(points[:, None], k[None, :], ph[None, :]))
         out["dlo"] = np.ascontiguousarray(np.stack([cos_family(0.0, k, ph, o) for o in (1, 2)]))
         out["dhi"] = np.ascontiguousarray(np.stack([cos_family(1.0, k, ph, o) for o in (1, 2)]))
-    out["coords"] = np.ascontiguousarray(splitmix_uniform(seed, 4, m * B).reshape(m, B))
+    idx = np.arange(m, dtype=np.uint64)[:, None] * np.uint64(total) + lines[None, :]
+    out["coords"] = np.ascontiguousarray(splitmix_at(seed, 4, idx))
     return out
 
 

@@ -86,3 +86,32 @@ def test_two_rank_sharded_build_equals_single_rank():
     for p in procs:
         p.join(timeout=60)
     assert results == {0: True, 1: True}, results
+
+
+def test_bench_starts_ranks_and_shards_the_batch():
+    """`bench.py --gpus 2` starts two ranks itself (torchrun), each rank draws its contiguous shard
+    of the global batch, and rank 0 reports n_gpus = 2 with the time as the max over ranks. The CPU
+    stub runs the same rank code over gloo with a NumPy step in place of the kernels."""
+    import json
+    import subprocess
+    import sys
+
+    import numpy as np
+
+    from ddc_b200 import workloads as W
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lines = 96
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--gpus", "2", "--cpu-stub", "--steps", "2",
+                        "--warmup", "3", "--lines", str(lines)], capture_output=True, text=True, timeout=240)
+    assert r.returncode == 0, r.stderr[-2000:]
+    out = [json.loads(ln) for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(out) == 1, r.stdout
+    line = out[0]
+    assert line["n_gpus"] == 2 and line["config"]["global_lines"] == 2 * lines
+    assert [s[:2] for s in line["shards"]] == [[0, lines], [lines, 2 * lines]]
+    # each rank's inputs are exactly its columns of the global batch
+    whole = W.config2(B=2 * lines, m=64, points=np.linspace(0.0, 1.0, 33))
+    for (a, b, check) in line["shards"]:
+        expect = float(whole["vals"][:, a:b].sum() + whole["coords"][:, a:b].sum())
+        assert abs(check - expect) <= 1e-9 * abs(expect)
