@@ -6,12 +6,13 @@ of include/ddcb.h; this package is the host-side mirror of the reference's splin
 from . import _lib
 from ._lib import DdcbError
 from .splines import (BSplines, Extrapolation, HostPipeline, NonUniformBSplines, SplineBuilder, SplineBuilder2D,
-                      SplineBuilderClosure, SplineEvaluator, SplineEvaluator2D, UnevenBatch, UniformBSplines,
-                      greville_points, lines_of, n_boundary_equations)
+                      SplineBuilder3D, SplineBuilderClosure, SplineEvaluator, SplineEvaluator2D, SplineEvaluator3D,
+                      SplineEvaluatorND, UnevenBatch, UniformBSplines, greville_points, lines_of, n_boundary_equations)
 
 __all__ = [
     "BSplines", "UniformBSplines", "NonUniformBSplines", "SplineBuilder", "SplineEvaluator", "SplineBuilder2D",
-    "SplineEvaluator2D", "SplineBuilderClosure", "UnevenBatch", "HostPipeline",
+    "SplineEvaluator2D", "SplineBuilder3D", "SplineEvaluator3D", "SplineEvaluatorND", "SplineBuilderClosure",
+    "UnevenBatch", "HostPipeline",
     "Extrapolation", "greville_points", "lines_of", "n_boundary_equations", "DdcbError", "load_library",
 ]
 

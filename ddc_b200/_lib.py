@@ -85,6 +85,8 @@ SIGNATURES = {
     "ddcb_build": [_vp, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp],
     "ddcb_solve_multirhs": [_vp, _vp, C.c_int64, C.c_int64, C.c_int32, _vp],
     "ddcb_quadrature_coefficients": [_vp, _vp, _vp, _vp],
+    "ddcb_quadrature_coefficients_device": [_vp, _vp, _vp],
+    "ddcb_integrate_samples": [_vp, _vp, C.c_int64, _vp, Lines, _vp, Lines, _vp, Lines, _vp],
     "ddcb_evaluator_create": [_vp, C.c_int, C.c_int, _pp],
     "ddcb_evaluator_destroy": [_vp],
     "ddcb_eval": [_vp, _vp, Lines, _vp, Lines, _vp, Lines, _vp],
@@ -103,6 +105,10 @@ SIGNATURES = {
     "ddcb_build2d": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int64, _vp, C.c_uint64, _vp],
     "ddcb_eval2d": [_vp, _vp, C.c_int32, C.c_int32, _vp, _vp, _vp, C.c_int64, C.c_int64, _vp],
     "ddcb_integrate2d": [_vp, _vp, _vp, _vp, C.c_int64, _vp],
+    "ddcb_build3d_workspace_bytes": [_vp, _vp, _vp, C.c_int64, C.POINTER(C.c_uint64)],
+    "ddcb_build3d": [_vp, _vp, _vp, _vp, _vp, C.c_int64, _vp, C.c_uint64, _vp],
+    "ddcb_evalnd": [_vp, C.c_int32, _vp, _vp, _vp, _vp, C.c_int64, C.c_int64, _vp],
+    "ddcb_integratend": [_vp, C.c_int32, _vp, _vp, C.c_int64, _vp],
     "ddcb_build_eval": [_vp, _vp, C.c_int32, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines,
                         C.POINTER(C.c_int32), _vp],
     "ddcb_build_adjoint": [_vp, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp],

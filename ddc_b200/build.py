@@ -13,7 +13,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libddcb.so")
 SOURCES = ["api.cu", "plan.cpp", "build_kernels.cu", "eval_kernels.cu", "fused_kernels.cu", "tensor2d.cu",
            "adjoint_kernels.cu", "refine_kernels.cu",
-           "uneven_batch.cu", "host_pipeline.cu"]
+           "uneven_batch.cu", "host_pipeline.cu", "quadrature.cu", "tensornd.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

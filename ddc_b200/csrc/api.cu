@@ -4,6 +4,9 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <vector>
+
+#include <nvtx3/nvToolsExt.h>
 
 #include "ddcb_internal.hpp"
 
@@ -24,9 +27,18 @@ namespace {
 
 thread_local std::string g_last_error;
 
-template <class F>
-ddcb_status guarded(F&& f)
+// An NVTX range named after the entry point spans each call (the reference labels its regions the
+// same way, e.g. spline_builder.hpp:1043), so profilers show the C-ABI calls around their kernels.
+struct NvtxRange
 {
+    explicit NvtxRange(char const* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
+
+template <class F>
+ddcb_status guarded(char const* name, F&& f)
+{
+    NvtxRange const range(name);
     try {
         f();
         g_last_error.clear();
@@ -178,7 +190,7 @@ const char* ddcb_last_error_message(void) { return g_last_error.c_str(); }
 ddcb_status ddcb_bsplines_create_uniform(int32_t degree, int32_t periodic, double rmin, double rmax, int64_t ncells,
                                          ddcb_bsplines* out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(out != nullptr, "out is NULL");
         auto* h = new ddcb_bsplines_t();
         try {
@@ -194,7 +206,7 @@ ddcb_status ddcb_bsplines_create_uniform(int32_t degree, int32_t periodic, doubl
 ddcb_status ddcb_bsplines_create_non_uniform(int32_t degree, int32_t periodic, const double* breaks, int64_t nbreaks,
                                              ddcb_bsplines* out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(out != nullptr, "out is NULL");
         auto* h = new ddcb_bsplines_t();
         try {
@@ -209,7 +221,7 @@ ddcb_status ddcb_bsplines_create_non_uniform(int32_t degree, int32_t periodic, c
 
 ddcb_status ddcb_bsplines_destroy(ddcb_bsplines b)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         if (!b) return;
         ddcb::free_basis(b->basis);
         delete b;
@@ -218,7 +230,7 @@ ddcb_status ddcb_bsplines_destroy(ddcb_bsplines b)
 
 ddcb_status ddcb_bsplines_get_info(ddcb_bsplines b, ddcb_bsplines_info* info)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(b && info, "NULL argument");
         auto const& d = b->basis.desc;
         info->degree = d.degree;
@@ -234,7 +246,7 @@ ddcb_status ddcb_bsplines_get_info(ddcb_bsplines b, ddcb_bsplines_info* info)
 
 ddcb_status ddcb_bsplines_knots(ddcb_bsplines b, int64_t first, int64_t count, double* out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(b && out, "NULL argument");
         require(first >= 0 && count >= 0 && first + count <= int64_t(b->basis.knots.size()), "knot range out of bounds");
         std::copy(b->basis.knots.begin() + first, b->basis.knots.begin() + first + count, out);
@@ -244,7 +256,7 @@ ddcb_status ddcb_bsplines_knots(ddcb_bsplines b, int64_t first, int64_t count, d
 ddcb_status ddcb_greville_points(ddcb_bsplines b, ddcb_closure lo, ddcb_closure hi, double* points, int64_t capacity,
                                  int64_t* npoints)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(b && npoints, "NULL argument");
         auto pts = ddcb::greville_points(b->basis, int(lo), int(hi));
         *npoints = int64_t(pts.size());
@@ -257,7 +269,7 @@ ddcb_status ddcb_greville_points(ddcb_bsplines b, ddcb_closure lo, ddcb_closure 
 
 ddcb_status ddcb_bsplines_integrals(ddcb_bsplines b, double* out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(b && out, "NULL argument");
         ddcb::basis_integrals(b->basis, out);
     });
@@ -266,12 +278,20 @@ ddcb_status ddcb_bsplines_integrals(ddcb_bsplines b, double* out)
 ddcb_status ddcb_builder_create(ddcb_bsplines basis, const double* interp_points, int64_t npoints, ddcb_closure lo,
                                 ddcb_closure hi, const ddcb_builder_options* options, ddcb_builder* out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(basis && out, "NULL argument");
         auto* h = new ddcb_builder_t();
         try {
             h->b = ddcb::create_builder(basis->basis, interp_points, long(npoints), int(lo), int(hi), options);
         } catch (...) {
+            delete h;
+            throw;
+        }
+        try {
+            // the quadrature weights, by the device transposed solve
+            ddcb::compute_device_quadrature(*h->b, h->b->d_quad_scratch, h->b->d_quad);
+        } catch (...) {
+            ddcb::destroy_builder(h->b);
             delete h;
             throw;
         }
@@ -281,7 +301,7 @@ ddcb_status ddcb_builder_create(ddcb_bsplines basis, const double* interp_points
 
 ddcb_status ddcb_builder_destroy(ddcb_builder b)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         if (!b) return;
         ddcb::destroy_builder(b->b);
         delete b;
@@ -290,7 +310,7 @@ ddcb_status ddcb_builder_destroy(ddcb_builder b)
 
 ddcb_status ddcb_builder_get_info(ddcb_builder h, ddcb_builder_info* info)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(h && info, "NULL argument");
         ddcb::Builder const& b = *h->b;
         info->nbasis = b.n;
@@ -348,7 +368,7 @@ ddcb_status ddcb_build_eval(ddcb_builder h, ddcb_evaluator he, int32_t order, do
                             ddcb_lines lhi, const double* coords, ddcb_lines lx, double* out, ddcb_lines lo,
                             int32_t* fused, ddcb_stream stream)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         if (fused) *fused = 0;
         require(he != nullptr, "evaluator is NULL");
         ddcb::Evaluator const& e = *he->e;
@@ -378,7 +398,7 @@ ddcb_status ddcb_build_eval(ddcb_builder h, ddcb_evaluator he, int32_t order, do
 ddcb_status ddcb_build(ddcb_builder h, double* coefs, ddcb_lines lc, const double* vals, ddcb_lines lv,
                        const double* dlo, ddcb_lines llo, const double* dhi, ddcb_lines lhi, ddcb_stream stream)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         if (!check_build(h, coefs, lc, vals, lv, dlo, llo, dhi, lhi)) return;
         ddcb::Builder const& b = *h->b;
         ddcb::launch_build(b, coefs, ddcb::to_lines(lc), vals, ddcb::to_lines(lv), dlo, ddcb::to_lines(llo), dhi,
@@ -389,7 +409,7 @@ ddcb_status ddcb_build(ddcb_builder h, double* coefs, ddcb_lines lc, const doubl
 ddcb_status ddcb_solve_multirhs(ddcb_builder h, double* rhs, int64_t ld, int64_t nrhs, int32_t transpose,
                                 ddcb_stream stream)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(h != nullptr, "builder is NULL");
         require(nrhs >= 0 && ld >= nrhs, "ld must be >= nrhs");
         if (nrhs == 0) return;
@@ -398,21 +418,71 @@ ddcb_status ddcb_solve_multirhs(ddcb_builder h, double* rhs, int64_t ld, int64_t
     });
 }
 
+static void check_device(int device, char const* what);
+
 ddcb_status ddcb_quadrature_coefficients(ddcb_builder h, double* qlo, double* q, double* qhi)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(h != nullptr, "builder is NULL");
         ddcb::Builder const& b = *h->b;
         require(q != nullptr, "q is NULL");
         require(b.nbv_lo == 0 || qlo != nullptr, "q_derivs_lo is NULL");
         require(b.nbv_hi == 0 || qhi != nullptr, "q_derivs_hi is NULL");
-        ddcb::builder_quadrature(b, qlo, q, qhi);
+        check_device(b.device, "builder");
+        std::vector<double> all(size_t(b.n));
+        DDCB_CUDA_CHECK(cudaMemcpy(all.data(), b.d_quad, sizeof(double) * all.size(), cudaMemcpyDeviceToHost));
+        long const nv = b.n - b.nbv_lo - b.nbv_hi;
+        std::copy(all.begin(), all.begin() + b.nbv_lo, qlo);
+        std::copy(all.begin() + b.nbv_lo, all.begin() + b.nbv_lo + nv, q);
+        std::copy(all.begin() + b.nbv_lo + nv, all.end(), qhi);
+    });
+}
+
+ddcb_status ddcb_quadrature_coefficients_device(ddcb_builder h, double* q_all, ddcb_stream stream)
+{
+    return guarded(__func__, [&] {
+        require(h != nullptr, "builder is NULL");
+        require(q_all != nullptr, "q_all is NULL");
+        ddcb::Builder const& b = *h->b;
+        check_device(b.device, "builder");
+        DDCB_CUDA_CHECK(cudaMemcpyAsync(q_all, b.d_quad, sizeof(double) * size_t(b.n), cudaMemcpyDeviceToDevice,
+                                        reinterpret_cast<cudaStream_t>(stream)));
+    });
+}
+
+ddcb_status ddcb_integrate_samples(ddcb_builder h, double* out, int64_t out_outer_stride, const double* vals,
+                                   ddcb_lines lv, const double* dlo, ddcb_lines llo, const double* dhi, ddcb_lines lhi,
+                                   ddcb_stream stream)
+{
+    return guarded(__func__, [&] {
+        require(h != nullptr, "builder is NULL");
+        ddcb::Builder const& b = *h->b;
+        check_device(b.device, "builder");
+        check_lines(lv, int64_t(b.points.size()), "vals");
+        int64_t const nl = lv.inner * lv.outer;
+        if (nl == 0) return;
+        require(vals != nullptr && out != nullptr, "vals or out is NULL");
+        require(lv.outer <= 1 || out_outer_stride >= lv.inner, "out_outer_stride must be >= the inner batch extent");
+        bool const her_lo = b.lo == DDCB_HERMITE && b.nbv_lo > 0, her_hi = b.hi == DDCB_HERMITE && b.nbv_hi > 0;
+        if (her_lo) {
+            require(dlo != nullptr, "derivs_lo is NULL but the lower closure is HERMITE");
+            check_lines(llo, b.nbv_lo, "derivs_lo");
+            same_batch(lv, llo, "derivs_lo");
+        }
+        if (her_hi) {
+            require(dhi != nullptr, "derivs_hi is NULL but the upper closure is HERMITE");
+            check_lines(lhi, b.nbv_hi, "derivs_hi");
+            same_batch(lv, lhi, "derivs_hi");
+        }
+        ddcb::launch_integrate_samples(b, out, out_outer_stride, vals, ddcb::to_lines(lv), her_lo ? dlo : nullptr,
+                                       ddcb::to_lines(llo), her_hi ? dhi : nullptr, ddcb::to_lines(lhi),
+                                       reinterpret_cast<cudaStream_t>(stream));
     });
 }
 
 ddcb_status ddcb_evaluator_create(ddcb_bsplines basis, ddcb_extrapolation lo, ddcb_extrapolation hi, ddcb_evaluator* out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(basis && out, "NULL argument");
         require(lo >= DDCB_EXTRAP_PERIODIC && lo <= DDCB_EXTRAP_CONSTANT && hi >= DDCB_EXTRAP_PERIODIC && hi <= DDCB_EXTRAP_CONSTANT,
                 "unknown extrapolation rule");
@@ -429,7 +499,7 @@ ddcb_status ddcb_evaluator_create(ddcb_bsplines basis, ddcb_extrapolation lo, dd
 
 ddcb_status ddcb_evaluator_destroy(ddcb_evaluator e)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         if (!e) return;
         ddcb::destroy_evaluator(e->e);
         delete e;
@@ -458,13 +528,13 @@ static void eval_common(ddcb_evaluator h, int order, double* out, ddcb_lines lo,
 ddcb_status ddcb_eval(ddcb_evaluator h, double* out, ddcb_lines lo, const double* coords, ddcb_lines lx,
                       const double* coefs, ddcb_lines lc, ddcb_stream stream)
 {
-    return guarded([&] { eval_common(h, 0, out, lo, coords, lx, coefs, lc, stream); });
+    return guarded(__func__, [&] { eval_common(h, 0, out, lo, coords, lx, coefs, lc, stream); });
 }
 
 ddcb_status ddcb_eval_deriv(ddcb_evaluator h, int32_t order, double* out, ddcb_lines lo, const double* coords,
                             ddcb_lines lx, const double* coefs, ddcb_lines lc, ddcb_stream stream)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(h != nullptr, "evaluator is NULL");
         require(order >= 1 && order <= h->e->basis.desc.degree, "derivative order must be in 1..degree");
         eval_common(h, order, out, lo, coords, lx, coefs, lc, stream);
@@ -474,7 +544,7 @@ ddcb_status ddcb_eval_deriv(ddcb_evaluator h, int32_t order, double* out, ddcb_l
 ddcb_status ddcb_integrate(ddcb_evaluator h, double* out, int64_t out_outer_stride, const double* coefs, ddcb_lines lc,
                            ddcb_stream stream)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(h != nullptr, "evaluator is NULL");
         ddcb::Evaluator const& e = *h->e;
         check_lines(lc, e.basis.size(), "coefs");
@@ -513,7 +583,7 @@ static void check_device(int device, char const* what)
 ddcb_status ddcb_build_adjoint(ddcb_builder h, const double* gc, ddcb_lines lgc, double* gv, ddcb_lines lgv,
                                double* gdlo, ddcb_lines lglo, double* gdhi, ddcb_lines lghi, ddcb_stream stream)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(h != nullptr, "builder is NULL");
         ddcb::Builder const& b = *h->b;
         check_lines(lgv, int64_t(b.points.size()), "g_vals");
@@ -552,7 +622,7 @@ ddcb_status ddcb_eval_adjoint(ddcb_evaluator he, int32_t order, const double* co
                               ddcb_lines lc, const double* gy, ddcb_lines lgy, double* gc, ddcb_lines lgc, double* gx,
                               ddcb_lines lgx, ddcb_stream stream)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(he != nullptr, "evaluator is NULL");
         ddcb::Evaluator const& e = *he->e;
         check_lines(lgc, e.basis.size(), "g_coefs");
@@ -570,7 +640,7 @@ ddcb_status ddcb_build_eval_adjoint(ddcb_builder h, ddcb_evaluator he, int32_t o
                                     double* gv, ddcb_lines lgv, double* gdlo, ddcb_lines lglo, double* gdhi,
                                     ddcb_lines lghi, double* gx, ddcb_lines lgx, int32_t* fused, ddcb_stream stream)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         if (fused) *fused = 0;
         require(h != nullptr, "builder is NULL");
         require(he != nullptr, "evaluator is NULL");
@@ -602,7 +672,7 @@ struct ddcb_uneven_batch_t
 ddcb_status ddcb_batch_uneven_create(const ddcb_builder* builders, const ddcb_evaluator* evaluators, const int64_t* nevals,
                                      int64_t count, ddcb_uneven_batch* out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(out != nullptr, "out is NULL");
         *out = nullptr;
         require(count >= 0 && count < (int64_t(1) << 30), "bad problem count");
@@ -627,7 +697,7 @@ ddcb_status ddcb_batch_uneven_create(const ddcb_builder* builders, const ddcb_ev
 
 ddcb_status ddcb_batch_uneven_destroy(ddcb_uneven_batch h)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         if (!h) return;
         ddcb::destroy_uneven_batch(h->b);
         delete h;
@@ -636,7 +706,7 @@ ddcb_status ddcb_batch_uneven_destroy(ddcb_uneven_batch h)
 
 ddcb_status ddcb_batch_uneven_get_info(ddcb_uneven_batch h, ddcb_uneven_info* info)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(h != nullptr && info != nullptr, "NULL argument");
         int64_t tot[6];
         int sch[4];
@@ -659,7 +729,7 @@ ddcb_status ddcb_batch_uneven_get_info(ddcb_uneven_batch h, ddcb_uneven_info* in
 ddcb_status ddcb_batch_uneven_offsets(ddcb_uneven_batch h, int64_t* vals, int64_t* dlo, int64_t* dhi, int64_t* coefs,
                                       int64_t* evals)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(h != nullptr, "batch is NULL");
         ddcb::uneven_offsets(*h->b, vals, dlo, dhi, coefs, evals);
     });
@@ -683,7 +753,7 @@ static void check_uneven_buffers(ddcb_uneven_batch h, const double* vals, const 
 ddcb_status ddcb_batch_uneven_tune(ddcb_uneven_batch h, const double* vals, const double* dlo, const double* dhi,
                                    double* coefs, const double* coords, double* out, int32_t reps, ddcb_stream stream)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         check_uneven_buffers(h, vals, dlo, dhi, coefs, coords, out);
         ddcb::tune_uneven_batch(*h->b, vals, dlo, dhi, coefs, coords, out, reps, reinterpret_cast<cudaStream_t>(stream));
     });
@@ -692,7 +762,7 @@ ddcb_status ddcb_batch_uneven_tune(ddcb_uneven_batch h, const double* vals, cons
 ddcb_status ddcb_batch_uneven_run(ddcb_uneven_batch h, const double* vals, const double* dlo, const double* dhi,
                                   double* coefs, const double* coords, double* out, ddcb_stream stream)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         check_uneven_buffers(h, vals, dlo, dhi, coefs, coords, out);
         ddcb::run_uneven_batch(*h->b, vals, dlo, dhi, coefs, coords, out, reinterpret_cast<cudaStream_t>(stream));
     });
@@ -719,7 +789,7 @@ static void check_host_layout(ddcb_lines const& l, char const* name)
 ddcb_status ddcb_host_pipeline_create(ddcb_builder hb, ddcb_evaluator he, int32_t order, int64_t npoints, int64_t slice_lines,
                                       ddcb_host_pipeline* out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(hb && he && out, "NULL argument");
         ddcb::Builder const& b = *hb->b;
         ddcb::Evaluator const& e = *he->e;
@@ -745,7 +815,7 @@ ddcb_status ddcb_host_pipeline_create(ddcb_builder hb, ddcb_evaluator he, int32_
 
 ddcb_status ddcb_host_pipeline_destroy(ddcb_host_pipeline h)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         if (!h) return;
         ddcb::destroy_host_pipeline(h->p);
         delete h;
@@ -756,7 +826,7 @@ ddcb_status ddcb_host_pipeline_run(ddcb_host_pipeline h, const double* vals, ddc
                                    const double* dhi, ddcb_lines lhi, const double* coords, ddcb_lines lx, double* out,
                                    ddcb_lines lo, double* coefs, ddcb_lines lc, ddcb_stream stream)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(h != nullptr, "pipeline is NULL");
         ddcb::HostPipeline& p = *h->p;
         ddcb::Builder const& b = *p.b;
@@ -815,7 +885,7 @@ ddcb_status ddcb_host_pipeline_run(ddcb_host_pipeline h, const double* vals, ddc
 
 ddcb_status ddcb_build2d_workspace_bytes(ddcb_builder b1, ddcb_builder b2, int64_t nbatch, uint64_t* bytes)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(b1 && b2 && bytes, "NULL argument");
         require(nbatch >= 0, "negative batch");
         *bytes = nbatch ? ddcb::build2d_workspace_bytes(*b1->b, *b2->b, nbatch) : 0;
@@ -827,7 +897,7 @@ ddcb_status ddcb_build2d(ddcb_builder h1, ddcb_builder h2, double* coefs, const 
                          const double* m21, const double* m12, const double* m22, int64_t nbatch, void* workspace,
                          uint64_t workspace_bytes, ddcb_stream stream)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(h1 && h2, "builder is NULL");
         require(nbatch >= 0, "negative batch");
         if (nbatch == 0) return;
@@ -873,7 +943,7 @@ ddcb_status ddcb_build2d(ddcb_builder h1, ddcb_builder h2, double* coefs, const 
 ddcb_status ddcb_eval2d(ddcb_evaluator h1, ddcb_evaluator h2, int32_t o1, int32_t o2, double* out, const double* coords,
                         const double* coefs, int64_t npoints, int64_t nbatch, ddcb_stream stream)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(h1 && h2, "evaluator is NULL");
         require(npoints >= 0 && nbatch >= 0, "negative size");
         require(o1 >= 0 && o1 <= 1 && o2 >= 0 && o2 <= 1, "2D derivative orders must be 0 or 1");
@@ -887,7 +957,7 @@ ddcb_status ddcb_eval2d(ddcb_evaluator h1, ddcb_evaluator h2, int32_t o1, int32_
 ddcb_status ddcb_integrate2d(ddcb_evaluator h1, ddcb_evaluator h2, double* out, const double* coefs, int64_t nbatch,
                              ddcb_stream stream)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(h1 && h2, "evaluator is NULL");
         require(nbatch >= 0, "negative batch");
         if (nbatch == 0) return;
@@ -903,7 +973,7 @@ ddcb_status ddcb_build2d_static_scratch(ddcb_builder h1, ddcb_builder h2, double
                                         const double* dmax2, const double* m11, const double* m21, const double* m12,
                                         const double* m22, int64_t nbatch, ddcb_stream stream)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         require(h1 && h2, "builder is NULL");
         require(nbatch >= 0, "negative batch");
         if (nbatch == 0) return;
@@ -927,6 +997,115 @@ ddcb_status ddcb_build2d_static_scratch(ddcb_builder h1, ddcb_builder h2, double
                                     h2lo ? dmin2 : nullptr, h2hi ? dmax2 : nullptr, (h1lo && h2lo) ? m11 : nullptr,
                                     (h1hi && h2lo) ? m21 : nullptr, (h1lo && h2hi) ? m12 : nullptr,
                                     (h1hi && h2hi) ? m22 : nullptr, nbatch, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+// ---- 3D builder and N-dimensional evaluator ---------------------------------------------------
+
+// Whether input k1 + 3 k2 + 9 k3 of a 3D build is read: every dimension with a derivative kind
+// (1 lower, 2 upper) has a HERMITE closure with derivative inputs on that side.
+static bool build3d_reads(ddcb::Builder const* const b[3], int idx)
+{
+    for (int d = 0; d < 3; ++d, idx /= 3) {
+        int const k = idx % 3;
+        if (k == 1 && !(b[d]->lo == DDCB_HERMITE && b[d]->nbv_lo > 0)) return false;
+        if (k == 2 && !(b[d]->hi == DDCB_HERMITE && b[d]->nbv_hi > 0)) return false;
+    }
+    return true;
+}
+
+ddcb_status ddcb_build3d_workspace_bytes(ddcb_builder b1, ddcb_builder b2, ddcb_builder b3, int64_t nbatch, uint64_t* bytes)
+{
+    return guarded(__func__, [&] {
+        require(b1 && b2 && b3 && bytes, "NULL argument");
+        require(nbatch >= 0, "negative batch");
+        *bytes = ddcb::build3d_workspace_bytes(*b1->b, *b2->b, *b3->b, nbatch);
+    });
+}
+
+ddcb_status ddcb_build3d(ddcb_builder h1, ddcb_builder h2, ddcb_builder h3, double* coefs, const double* const* inputs,
+                         int64_t nbatch, void* workspace, uint64_t workspace_bytes, ddcb_stream stream)
+{
+    return guarded(__func__, [&] {
+        require(h1 && h2 && h3, "builder is NULL");
+        require(nbatch >= 0, "negative batch");
+        if (nbatch == 0) return;
+        require(coefs && inputs && inputs[0], "coefs / inputs / vals pointer is NULL");
+        ddcb::Builder const* const b[3] = {h1->b, h2->b, h3->b};
+        const double* in[27];
+        for (int i = 0; i < 27; ++i) {
+            bool const reads = build3d_reads(b, i);
+            in[i] = reads ? inputs[i] : nullptr;
+            if (reads && in[i] == nullptr)
+                throw ddcb::Error(DDCB_ERR_INVALID_ARGUMENT, "build3d: input " + std::to_string(i)
+                                                                 + " (k1 + 3 k2 + 9 k3) is required by the HERMITE closures");
+        }
+        int dev = 0;
+        DDCB_CUDA_CHECK(cudaGetDevice(&dev));
+        require(dev == b[0]->device && dev == b[1]->device && dev == b[2]->device, "the builders were created for another device");
+        size_t const need = ddcb::build3d_workspace_bytes(*b[0], *b[1], *b[2], nbatch);
+        cudaStream_t const s = reinterpret_cast<cudaStream_t>(stream);
+        void* ws = workspace;
+        bool owned = false;
+        if (ws == nullptr) {
+            DDCB_CUDA_CHECK(cudaMallocAsync(&ws, need, s));
+            owned = true;
+        } else {
+            require(workspace_bytes >= need, "workspace too small (see ddcb_build3d_workspace_bytes)");
+        }
+        try {
+            ddcb::launch_build3d(*b[0], *b[1], *b[2], coefs, in, nbatch, static_cast<double*>(ws), s);
+        } catch (...) {
+            if (owned) cudaFreeAsync(ws, s);
+            throw;
+        }
+        if (owned) DDCB_CUDA_CHECK(cudaFreeAsync(ws, s));
+    });
+}
+
+static void evaluators_nd(const ddcb_evaluator* evaluators, int32_t ndims, ddcb::Evaluator const** e)
+{
+    require(evaluators != nullptr, "evaluators is NULL");
+    require(ndims >= 1 && ndims <= ddcb::kMaxDims, "ndims must be in 1..6");
+    int dev = 0;
+    DDCB_CUDA_CHECK(cudaGetDevice(&dev));
+    for (int d = 0; d < ndims; ++d) {
+        require(evaluators[d] != nullptr, "evaluator is NULL");
+        e[d] = evaluators[d]->e;
+        require(e[d]->device == dev, "an evaluator was created for another device");
+    }
+}
+
+ddcb_status ddcb_evalnd(const ddcb_evaluator* evaluators, int32_t ndims, const int32_t* orders, double* out,
+                        const double* coords, const double* coefs, int64_t npoints, int64_t nbatch, ddcb_stream stream)
+{
+    return guarded(__func__, [&] {
+        ddcb::Evaluator const* e[ddcb::kMaxDims] = {};
+        evaluators_nd(evaluators, ndims, e);
+        require(npoints >= 0 && nbatch >= 0, "negative size");
+        int ord[ddcb::kMaxDims] = {};
+        if (orders)
+            for (int d = 0; d < ndims; ++d) {
+                require(orders[d] >= 0 && orders[d] <= e[d]->basis.desc.degree, "derivative order outside 0..degree");
+                ord[d] = orders[d];
+            }
+        if (npoints == 0 || nbatch == 0) return;
+        require(out && coords && coefs, "NULL data pointer");
+        ddcb::launch_evalnd(e, ndims, orders ? ord : nullptr, out, coords, coefs, npoints, nbatch,
+                            reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+ddcb_status ddcb_integratend(const ddcb_evaluator* evaluators, int32_t ndims, double* out, const double* coefs,
+                             int64_t nbatch, ddcb_stream stream)
+{
+    return guarded(__func__, [&] {
+        ddcb::Evaluator const* e[ddcb::kMaxDims] = {};
+        evaluators_nd(evaluators, ndims, e);
+        require(nbatch >= 0, "negative batch");
+        if (nbatch == 0) return;
+        require(out && coefs, "NULL data pointer");
+        ddcb::launch_integratend(e, ndims, out, coefs, nbatch, reinterpret_cast<cudaStream_t>(stream));
     });
 }
 

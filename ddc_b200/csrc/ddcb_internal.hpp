@@ -162,6 +162,9 @@ struct Builder
     SolveTables tables_t {};       // tables of A^T (adjoint)
     void* d_block = nullptr;       // one allocation holding every device table
     size_t d_block_bytes = 0;
+    double* d_quad = nullptr;      // quadrature weights (n, reference row order, Hermite rows scaled
+                                   // by dx^k), computed on the device at creation; inside d_block
+    double* d_quad_scratch = nullptr; // n doubles of d_block for that computation
     RhsMap rhs {};
     std::string structure;
     void* host_private = nullptr;  // host factorisation (plan.cpp)
@@ -195,7 +198,14 @@ void upload_builder(Builder* b);
 double emulate_device_solve(Builder const& b, double const* rhs, bool transpose);
 double emulate_build(Builder const& b, double const* vals, double const* dlo, double const* dhi);
 void destroy_builder(Builder* b);
-void builder_quadrature(Builder const& b, double* qlo, double* q, double* qhi);
+// Most dimensions of a tensor-product evaluation (SplineEvaluatorND).
+constexpr int kMaxDims = 6;
+
+// quadrature.cu: weights by the device transposed solve (d_qk: n doubles of scratch), and the
+// integral of the interpolating spline of every line straight from its samples.
+void compute_device_quadrature(Builder& b, double* d_qk, double* d_q);
+void launch_integrate_samples(Builder const& b, double* out, int64_t out_outer_stride, double const* vals, Lines const& lv,
+                              double const* dlo, Lines const& llo, double const* dhi, Lines const& lhi, cudaStream_t s);
 
 // build_kernels.cu
 void launch_build(Builder const& b, double* coefs, Lines const& lc, double const* vals, Lines const& lv,
@@ -274,6 +284,15 @@ void launch_build2d(Builder const& b1, Builder const& b2, double* coefs, double 
 void launch_eval2d(Evaluator const& e1, Evaluator const& e2, int o1, int o2, double* out, double const* coords,
                    double const* coefs, int64_t m, int64_t B, cudaStream_t s);
 void launch_integrate2d(Evaluator const& e1, Evaluator const& e2, double* out, double const* coefs, int64_t B, cudaStream_t s);
+
+// tensornd.cu: 3D builder (inputs: 27 arrays, index k1 + 3 k2 + 9 k3 with k = 0 values, 1 lower,
+// 2 upper derivatives along that dimension) and the N-dimensional evaluator / integrator.
+size_t build3d_workspace_bytes(Builder const& b1, Builder const& b2, Builder const& b3, int64_t B);
+void launch_build3d(Builder const& b1, Builder const& b2, Builder const& b3, double* coefs, double const* const* inputs,
+                    int64_t B, double* ws, cudaStream_t s);
+void launch_evalnd(Evaluator const* const* e, int ndims, int const* orders, double* out, double const* coords,
+                   double const* coefs, int64_t m, int64_t B, cudaStream_t s);
+void launch_integratend(Evaluator const* const* e, int ndims, double* out, double const* coefs, int64_t B, cudaStream_t s);
 size_t build2d_static_scratch_bytes();
 void launch_build2d_static(Builder const& b1, Builder const& b2, double* coefs, double const* vals, double const* dmin1,
                            double const* dmax1, double const* dmin2, double const* dmax2, double const* m11,

@@ -1052,11 +1052,16 @@ void upload_builder(Builder* b)
     std::vector<size_t> offs_f, offs_a;
     b->tables = upload_tables(priv->fwd, blob, offs_f);
     b->tables_t = upload_tables(priv->adj, blob, offs_a);
+    // the quadrature weights and their scratch (2 n doubles) follow the tables
+    size_t const qoff = (blob.size() + 255) & ~size_t(255);
+    blob.resize(qoff + 2 * sizeof(double) * size_t(b->n), 0);
     DDCB_CUDA_CHECK(cudaMalloc(&b->d_block, blob.size()));
     DDCB_CUDA_CHECK(cudaMemcpy(b->d_block, blob.data(), blob.size(), cudaMemcpyHostToDevice));
     b->d_block_bytes = blob.size();
     bind_tables(b->tables, static_cast<char*>(b->d_block), offs_f.data());
     bind_tables(b->tables_t, static_cast<char*>(b->d_block), offs_a.data());
+    b->d_quad_scratch = reinterpret_cast<double*>(static_cast<char*>(b->d_block) + qoff);
+    b->d_quad = b->d_quad_scratch + b->n;
 }
 
 Builder* create_builder(Basis const& basis, double const* pts, long npts, int lo, int hi, ddcb_builder_options const* opts)
@@ -1291,28 +1296,6 @@ void destroy_builder(Builder* b)
     if (b->d_block) cudaFree(b->d_block);
     free_basis(b->basis);
     delete b;
-}
-
-// quadrature_coefficients (spline_builder.hpp:1103-1234): solve A^T q = integrals, un-rotate the
-// periodic offset, split into Hermite / value parts and scale the Hermite parts by dx^k.
-void builder_quadrature(Builder const& b, double* qlo, double* q, double* qhi)
-{
-    HostSolve const& h = static_cast<BuilderPrivate const*>(b.host_private)->fwd;
-    std::vector<double> ints(b.basis.size());
-    basis_integrals(b.basis, ints.data());
-    // As the reference does, the right-hand side is integral_bsplines in basis order (entry j is
-    // the integral of B-spline j), without the periodic column rotation.
-    // A^T q = ints in reference order; in kernel order (rows rotated by rrot, cols by crot) the
-    // transposed system reads its right-hand side rotated by crot and returns q rotated by rrot.
-    long const nn = b.n;
-    std::vector<double> rk(nn), rhs(nn);
-    for (long j = 0; j < nn; ++j) rk[j] = ints[(j + b.crot) % nn];
-    h.solve_host(rk.data(), true);
-    for (long i = 0; i < nn; ++i) rhs[(i + b.rrot) % nn] = rk[i];
-    long const nv = b.n - b.nbv_lo - b.nbv_hi;
-    for (int i = 0; i < b.nbv_lo; ++i) qlo[i] = rhs[i] * ipow(b.dx, i + b.odd);
-    for (long i = 0; i < nv; ++i) q[i] = rhs[b.nbv_lo + i];
-    for (int i = 0; i < b.nbv_hi; ++i) qhi[i] = rhs[b.nbv_lo + nv + i] * ipow(b.dx, i + b.odd);
 }
 
 } // namespace ddcb

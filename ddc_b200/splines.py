@@ -284,6 +284,31 @@ class SplineBuilder:
                   q.ctypes.data_as(C.c_void_p), qhi.ctypes.data_as(C.c_void_p))
         return qlo[: self.s_nbv_xmin], q, qhi[: self.s_nbv_xmax]
 
+    def quadrature_coefficients_device(self, stream=None):
+        """The quadrature weights as one CUDA float64 tensor of nbasis entries, [q_derivs_xmin, q,
+        q_derivs_xmax] (quadrature_coefficients<OutMemorySpace>() with a device memory space)."""
+        import torch
+
+        out = torch.empty(self.info.nbasis, dtype=torch.float64, device="cuda")
+        _lib.call("ddcb_quadrature_coefficients_device", self._h, _ptr(out), _stream_handle(stream))
+        return out
+
+    def integrate_samples(self, integrals, vals, derivs_xmin=None, derivs_xmax=None, *, dim: int = 0, stream=None):
+        """The integral of the spline interpolating each batch line of vals (and its Hermite
+        derivatives): operator() then SplineEvaluator::integrate in one pass over the samples.
+        integrals has the batch shape of vals."""
+        out = _dev_f64(integrals, "integrals")
+        vals = _dev_f64(vals, "vals")
+        dlo = _dev_f64(derivs_xmin, "derivs_xmin")
+        dhi = _dev_f64(derivs_xmax, "derivs_xmax")
+        lv = lines_of(vals, dim)
+        assert out.numel() == lv.inner * lv.outer and out.is_contiguous()
+        llo = lines_of(dlo, dim) if dlo is not None else Lines(0, 1, 0, 0, 0)
+        lhi = lines_of(dhi, dim) if dhi is not None else Lines(0, 1, 0, 0, 0)
+        _lib.call("ddcb_integrate_samples", self._h, _ptr(out), lv.inner, _ptr(vals), lv, _ptr(dlo), llo, _ptr(dhi), lhi,
+                  _stream_handle(stream))
+        return out
+
 
 class SplineEvaluator:
     """ddc::SplineEvaluator<..., LowerExtrapolationRule, UpperExtrapolationRule>."""
@@ -530,3 +555,107 @@ class HostPipeline:
                   lines_of(out, dim), _ptr(coefs), lines_of(coefs, dim) if coefs is not None else empty,
                   _stream_handle(stream))
         return spline_eval
+
+
+class SplineBuilder3D:
+    """ddc::SplineBuilder3D over three 1D builders (spline_builder_3d.hpp:597-1126).
+
+    Data layout (x1, x2, x3, batch...) with the batch contiguous: vals (np1, np2, np3, *batch) ->
+    spline (size1, size2, size3, *batch). Derivative arrays are passed by the reference's names;
+    each has the rows of its derivative kind along the dimensions it names and the interpolation
+    points along the others (e.g. derivs_min2: (np1, nbv_lo2, np3, *batch)).
+    """
+
+    # reference argument name -> (k1, k2, k3) with k = 0 values, 1 lower, 2 upper derivatives
+    KINDS = {"derivs_min1": (1, 0, 0), "derivs_max1": (2, 0, 0), "derivs_min2": (0, 1, 0), "derivs_max2": (0, 2, 0),
+             "derivs_min3": (0, 0, 1), "derivs_max3": (0, 0, 2)}
+    for _a, _i in (("min", 1), ("max", 2)):
+        for _b, _j in (("min", 1), ("max", 2)):
+            KINDS[f"mixed_derivs_{_a}1_{_b}2"] = (_i, _j, 0)
+            KINDS[f"mixed_derivs_{_a}2_{_b}3"] = (0, _i, _j)
+            KINDS[f"mixed_derivs_{_a}1_{_b}3"] = (_i, 0, _j)
+            for _c, _k in (("min", 1), ("max", 2)):
+                KINDS[f"mixed_derivs_{_a}1_{_b}2_{_c}3"] = (_i, _j, _k)
+
+    def __init__(self, builder1: SplineBuilder, builder2: SplineBuilder, builder3: SplineBuilder):
+        self.builders = (builder1, builder2, builder3)
+
+    def workspace_bytes(self, nbatch: int) -> int:
+        out = C.c_uint64()
+        _lib.call("ddcb_build3d_workspace_bytes", *[b._h for b in self.builders], int(nbatch), C.byref(out))
+        return out.value
+
+    def __call__(self, spline, vals, *, workspace=None, stream=None, **derivs):
+        spline = _dev_f64(spline, "spline")
+        vals = _dev_f64(vals, "vals")
+        assert spline.is_contiguous() and vals.is_contiguous()
+        nbatch = vals[0, 0, 0].numel()
+        ptrs = (C.c_void_p * 27)()
+        ptrs[0] = vals.data_ptr()
+        keep = [vals]
+        for name, arr in derivs.items():
+            if name not in self.KINDS:
+                raise TypeError(f"unknown derivative argument {name}")
+            if arr is None:
+                continue
+            arr = _dev_f64(arr, name)
+            assert arr.is_contiguous()
+            k1, k2, k3 = self.KINDS[name]
+            ptrs[k1 + 3 * k2 + 9 * k3] = arr.data_ptr()
+            keep.append(arr)
+        ws_ptr, ws_bytes = C.c_void_p(0), 0
+        if workspace is not None:
+            ws_ptr, ws_bytes = C.c_void_p(workspace.data_ptr()), workspace.numel() * workspace.element_size()
+        _lib.call("ddcb_build3d", *[b._h for b in self.builders], _ptr(spline), C.cast(ptrs, C.c_void_p), int(nbatch),
+                  ws_ptr, ws_bytes, _stream_handle(stream))
+        return spline
+
+
+class SplineEvaluatorND:
+    """ddc::SplineEvaluatorND (spline_evaluator_nd.hpp) over N 1D evaluators (N in 1..6); with N = 3
+    it is ddc::SplineEvaluator3D. coords_eval: (*points, *batch, N) coordinate tuples;
+    spline_coef: (size_1, ..., size_N, *batch)."""
+
+    def __init__(self, *evaluators: SplineEvaluator):
+        if not 1 <= len(evaluators) <= 6:
+            raise ValueError("1 to 6 evaluators")
+        self.evaluators = tuple(evaluators)
+        self.ndims = len(evaluators)
+        self._handles = (C.c_void_p * self.ndims)(*[e._h.value for e in evaluators])
+
+    def _run(self, orders, spline_eval, coords_eval, spline_coef, stream):
+        out = _dev_f64(spline_eval, "spline_eval")
+        x = _dev_f64(coords_eval, "coords_eval")
+        c = _dev_f64(spline_coef, "spline_coef")
+        assert out.is_contiguous() and x.is_contiguous() and c.is_contiguous()
+        nbatch = c[(0,) * self.ndims].numel()
+        npoints = out.numel() // max(nbatch, 1)
+        assert x.numel() == self.ndims * out.numel()
+        o = None if orders is None else (C.c_int32 * self.ndims)(*[int(v) for v in orders])
+        _lib.call("ddcb_evalnd", C.cast(self._handles, C.c_void_p), self.ndims,
+                  C.cast(o, C.c_void_p) if o is not None else None, _ptr(out), _ptr(x), _ptr(c), int(npoints),
+                  int(nbatch), _stream_handle(stream))
+        return out
+
+    def __call__(self, spline_eval, coords_eval, spline_coef, *, stream=None):
+        """operator(): values with the periodic wraps and extrapolation rules."""
+        return self._run(None, spline_eval, coords_eval, spline_coef, stream)
+
+    def deriv(self, orders, spline_eval, coords_eval, spline_coef, *, stream=None):
+        """deriv(DiscreteElement<Deriv<X1>, ...>(orders...), ...): orders[d] in 0..degree_d."""
+        assert len(orders) == self.ndims
+        return self._run(orders, spline_eval, coords_eval, spline_coef, stream)
+
+    def integrate(self, integrals, spline_coef, *, stream=None):
+        out = _dev_f64(integrals, "integrals")
+        c = _dev_f64(spline_coef, "spline_coef")
+        nbatch = c[(0,) * self.ndims].numel()
+        assert out.numel() == nbatch and out.is_contiguous() and c.is_contiguous()
+        _lib.call("ddcb_integratend", C.cast(self._handles, C.c_void_p), self.ndims, _ptr(out), _ptr(c), int(nbatch),
+                  _stream_handle(stream))
+        return out
+
+
+def SplineEvaluator3D(evaluator1: SplineEvaluator, evaluator2: SplineEvaluator, evaluator3: SplineEvaluator):
+    """ddc::SplineEvaluator3D (spline_evaluator_3d.hpp): the N-dimensional evaluator with N = 3."""
+    return SplineEvaluatorND(evaluator1, evaluator2, evaluator3)

@@ -136,8 +136,22 @@ ddcb_status ddcb_build(ddcb_builder b, double* coefs, ddcb_lines coefs_layout, c
 ddcb_status ddcb_solve_multirhs(ddcb_builder b, double* rhs, int64_t ld, int64_t nrhs, int32_t transpose,
                                 ddcb_stream stream);
 /* SplineBuilder::quadrature_coefficients() (spline_builder.hpp:1103-1234), host outputs of
- * nbv_lo, nbasis - nbv_lo - nbv_hi and nbv_hi entries; the Hermite parts are scaled by dx^k. */
+ * nbv_lo, nbasis - nbv_lo - nbv_hi and nbv_hi entries; the Hermite parts are scaled by dx^k. The
+ * weights solve A^T q = integrals with the device's transposed solve, once, when the builder is
+ * created; this call copies them out (synchronously). */
 ddcb_status ddcb_quadrature_coefficients(ddcb_builder b, double* q_derivs_lo, double* q_vals, double* q_derivs_hi);
+/* The same weights as one device array of nbasis entries, [q_derivs_lo, q_vals, q_derivs_hi],
+ * copied stream-ordered into q_all (a device pointer): quadrature_coefficients<OutMemorySpace>()
+ * with a device memory space. */
+ddcb_status ddcb_quadrature_coefficients_device(ddcb_builder b, double* q_all, ddcb_stream stream);
+/* SplineBuilder::operator() followed by SplineEvaluator::integrate (spline_evaluator.hpp:493-526)
+ * on the same lines, fused: out[(b / inner)*out_outer_stride + b % inner] is the integral of the
+ * spline interpolating line b's samples (and Hermite derivatives, read as in ddcb_build), computed
+ * as the dot product of the samples with the quadrature weights -- one read of the samples, no
+ * coefficient array. */
+ddcb_status ddcb_integrate_samples(ddcb_builder b, double* out, int64_t out_outer_stride, const double* vals,
+                                   ddcb_lines vals_layout, const double* derivs_lo, ddcb_lines derivs_lo_layout,
+                                   const double* derivs_hi, ddcb_lines derivs_hi_layout, ddcb_stream stream);
 
 /* ---- evaluator: SplineEvaluator<..., LowerExtrapolationRule, UpperExtrapolationRule>
  *      (spline_evaluator.hpp:160-186). ------------------------------------------------------- */
@@ -295,6 +309,40 @@ ddcb_status ddcb_eval2d(ddcb_evaluator e1, ddcb_evaluator e2, int32_t order1, in
 /* SplineEvaluator2D::integrate (spline_evaluator_2d.hpp:616-660): out[b] = sum c(r1, r2, b) I1[r1] I2[r2]. */
 ddcb_status ddcb_integrate2d(ddcb_evaluator e1, ddcb_evaluator e2, double* out, const double* coefs, int64_t nbatch,
                              ddcb_stream stream);
+
+/* ---- 3D tensor product: SplineBuilder3D (spline_builder_3d.hpp:597-1126) on three 1D plans, for
+ *      the layout (x1, x2, x3, batch) with the batch contiguous. ------------------------------ */
+/* Workspace of ddcb_build3d: the results of the dimension-1 and dimension-2 passes. */
+ddcb_status ddcb_build3d_workspace_bytes(ddcb_builder b1, ddcb_builder b2, ddcb_builder b3, int64_t nbatch,
+                                         uint64_t* bytes);
+/* SplineBuilder3D::operator() (spline_builder_3d.hpp:934-1126): vals (np1, np2, np3, nbatch) ->
+ * coefs (size1, size2, size3, nbatch). inputs holds 27 pointers; inputs[k1 + 3*k2 + 9*k3] is the
+ * array whose dimension d holds values (k_d = 0, np_d rows), lower derivatives (k_d = 1, nbv_lo_d
+ * rows) or upper derivatives (k_d = 2, nbv_hi_d rows), shape (rows1, rows2, rows3, nbatch). So
+ * inputs[0] = vals, [1] / [2] = derivs_min1 / derivs_max1, [3] / [6] = derivs_min2 / derivs_max2,
+ * [9] / [18] = derivs_min3 / derivs_max3, [4] = mixed_derivs_min1_min2, [5] = max1_min2,
+ * [7] = min1_max2, [8] = max1_max2, [10] = min1_min3, [11] = max1_min3, [19] = min1_max3,
+ * [20] = max1_max3, [12] = min2_min3, [15] = max2_min3, [21] = min2_max3, [24] = max2_max3, and
+ * [13] = min1_min2_min3, [14], [16], [17], [22], [23], [25], [26] the other corners likewise. An
+ * array is read only when every dimension with a derivative kind has a HERMITE closure on that
+ * side (the others may be NULL). workspace: ddcb_build3d_workspace_bytes bytes of device memory,
+ * or NULL to have the call allocate it stream-ordered. */
+ddcb_status ddcb_build3d(ddcb_builder b1, ddcb_builder b2, ddcb_builder b3, double* coefs, const double* const* inputs,
+                         int64_t nbatch, void* workspace, uint64_t workspace_bytes, ddcb_stream stream);
+
+/* ---- N-dimensional evaluation: SplineEvaluatorND (spline_evaluator_nd.hpp:306-590) and, with
+ *      ndims = 3, SplineEvaluator3D (spline_evaluator_3d.hpp), over ndims (1..6) 1D evaluators;
+ *      coefs (size_1, ..., size_N, nbatch), coords (npoints, nbatch, ndims), out (npoints, nbatch). */
+/* orders == NULL: operator() -- periodic wraps, then the extrapolation rule of the first
+ * non-periodic dimension outside its domain (null: 0; constant: the value at that boundary with
+ * the other non-periodic coordinates clamped into their domains); else deriv(orders) with
+ * orders[d] in 0..degree_d and no boundary handling (eval_no_bc, spline_evaluator_nd.hpp:766-825). */
+ddcb_status ddcb_evalnd(const ddcb_evaluator* evaluators, int32_t ndims, const int32_t* orders, double* out,
+                        const double* coords, const double* coefs, int64_t npoints, int64_t nbatch, ddcb_stream stream);
+/* SplineEvaluatorND::integrate (spline_evaluator_nd.hpp:596-633): out[b] = sum over the coefficient
+ * grid of c(i_1, ..., i_N, b) prod_d integral(B_{i_d}). */
+ddcb_status ddcb_integratend(const ddcb_evaluator* evaluators, int32_t ndims, double* out, const double* coefs,
+                             int64_t nbatch, ddcb_stream stream);
 
 #ifdef __cplusplus
 }

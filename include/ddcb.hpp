@@ -6,7 +6,7 @@
 // turn every failing status into std::runtime_error carrying the library's message, the error
 // type the reference throws at construction (spline_builder.hpp:227-260). Data are device pointers
 // with a ddcb_lines layout; `lines_xb` and `lines_bx` build the two common ones. An adapter that
-// owns DDC ChunkSpans fills the layout from the span's extents and strides (INTEGRATION.md).
+// owns DDC ChunkSpans fills the layout from the span's extents and strides.
 #pragma once
 
 #include <stdexcept>

@@ -304,3 +304,99 @@ class LinearProblem:
         b = np.ascontiguousarray(b, dtype=np.float64).copy()
         lib().orc_lp_solve(self._h, _p(b), b.shape[1], int(transpose))
         return b
+
+
+def _apply1(builder, arr, dlo=None, dhi=None, nthreads=None):
+    """The 1D builder along axis 0 of arr (rows, *rest): returns (size, *rest)."""
+    rest = arr.shape[1:]
+    B = int(np.prod(rest)) if rest else 1
+    flat = lambda a: None if a is None else np.ascontiguousarray(a).reshape(a.shape[0], B)
+    out = builder(flat(arr), flat(dlo), flat(dhi), nthreads=nthreads)
+    return out.reshape((builder.bs.size,) + tuple(rest))
+
+
+def build3d(b1: Builder, b2: Builder, b3: Builder, vals, derivs=None, nthreads=None):
+    """SplineBuilder3D::operator() (spline_builder_3d.hpp:934-1126), the reference's schedule: builder
+    1 over the dimension-2 / dimension-3 derivative slabs and the (2, 3) mixed slabs, with the
+    mixed derivatives involving dimension 1 as its Hermite data (:944-1101), builder 1 over the
+    values (:1103-1110), then SplineBuilder2D over dimensions 2-3 with the results (:1112-1125),
+    whose batch is (size1, batch). vals (np1, np2, np3, B); derivs maps the reference's argument
+    names (derivs_min1, ..., mixed_derivs_max1_max2_max3) to arrays; returns (size1, size2, size3, B)."""
+    derivs = derivs or {}
+    g = lambda k: None if derivs.get(k) is None else np.ascontiguousarray(derivs[k], dtype=np.float64)
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    s1 = b1.bs.size
+    B = vals.shape[3]
+    her = lambda b, side: (b.lo if side == "min" else b.hi) == HERMITE
+
+    def slab(name, m1a, m1b, cond):
+        if not cond:
+            return None
+        return _apply1(b1, g(name), g(m1a), g(m1b), nthreads)
+
+    sd = {}
+    for s2 in ("min", "max"):
+        sd[f"2{s2}"] = slab(f"derivs_{s2}2", f"mixed_derivs_min1_{s2}2", f"mixed_derivs_max1_{s2}2", her(b2, s2))
+        sd[f"3{s2}"] = slab(f"derivs_{s2}3", f"mixed_derivs_min1_{s2}3", f"mixed_derivs_max1_{s2}3", her(b3, s2))
+    for s2 in ("min", "max"):
+        for s3 in ("min", "max"):
+            sd[f"23{s2}{s3}"] = slab(f"mixed_derivs_{s2}2_{s3}3", f"mixed_derivs_min1_{s2}2_{s3}3",
+                                     f"mixed_derivs_max1_{s2}2_{s3}3", her(b2, s2) and her(b3, s3))
+    spline1 = _apply1(b1, vals, g("derivs_min1"), g("derivs_max1"), nthreads)  # (s1, np2, np3, B)
+    # dimensions (2, 3) with the batch (s1, B)
+    to2d = lambda a: None if a is None else np.ascontiguousarray(np.moveaxis(a, 0, 2)).reshape(a.shape[1], a.shape[2], s1 * B)
+    out = build2d(b2, b3, to2d(spline1), to2d(sd["2min"]), to2d(sd["2max"]), to2d(sd["3min"]), to2d(sd["3max"]),
+                  (to2d(sd["23minmin"]), to2d(sd["23maxmin"]), to2d(sd["23minmax"]), to2d(sd["23maxmax"])), nthreads)
+    out = out.reshape(b2.bs.size, b3.bs.size, s1, B)
+    return np.ascontiguousarray(np.moveaxis(out, 2, 0))
+
+
+def evaluatend(bss, coords, coefs, orders=None, ex=None):
+    """SplineEvaluatorND: operator() (orders None; spline_evaluator_nd.hpp:636-720, periodic wraps,
+    then the rule of the first non-periodic dimension outside its domain -- null: 0, constant: the
+    value at that boundary with the other non-periodic coordinates clamped, the N-dimensional form
+    of ConstantExtrapolationRule<DimI, DimNI>, constant_extrapolation_rule.hpp:143-193) or
+    deriv(orders) (eval_no_bc, :766-825). coords (m, B, N); coefs (size_1, ..., size_N, B); ex: per
+    dimension (lower, upper) rule codes. A per-point loop: for small cases."""
+    N = len(bss)
+    coords = np.asarray(coords, dtype=np.float64)
+    m, B = coords.shape[:2]
+    ex = ex or [(EX_NULL, EX_NULL)] * N
+    out = np.zeros((m, B))
+    for p in range(m):
+        for b in range(B):
+            x = [float(v) for v in coords[p, b]]
+            if orders is None:
+                for d, bs in enumerate(bss):
+                    if bs.periodic and (x[d] < bs.rmin or x[d] > bs.rmax):
+                        L = bs.rmax - bs.rmin
+                        x[d] -= np.floor((x[d] - bs.rmin) / L) * L
+                zero = False
+                for d, bs in enumerate(bss):
+                    if bs.periodic or bs.rmin <= x[d] <= bs.rmax:
+                        continue
+                    low = x[d] < bs.rmin
+                    if ex[d][0 if low else 1] == EX_NULL:
+                        zero = True
+                    else:
+                        x[d] = bs.rmin if low else bs.rmax
+                        for e, be in enumerate(bss):
+                            if e != d and not be.periodic:
+                                x[e] = min(max(x[e], be.rmin), be.rmax)
+                    break
+                if zero:
+                    continue
+            jv = []
+            for d, bs in enumerate(bss):
+                o = 0 if orders is None else int(orders[d])
+                if o == 0:
+                    jv.append(bs.eval_basis(x[d]))
+                else:
+                    j, dv = bs.eval_basis_and_n_derivs(x[d], o)
+                    jv.append((j, dv[:, o]))
+            sub = coefs[tuple(slice(j, j + bs.degree + 1) for (j, _), bs in zip(jv, bss)) + (b,)]
+            w = jv[0][1]
+            for _, v in jv[1:]:
+                w = np.multiply.outer(w, v)
+            out[p, b] = float((sub * w).sum())
+    return out
