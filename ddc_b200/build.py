@@ -49,8 +49,15 @@ def build(verbose: bool = False, force: bool = False) -> str:
     if verbose:
         common.append("-Xptxas=-v")
 
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".hpp", ".h"))]
+    headers.append(os.path.join(HERE, "..", "include", "ddcb.h"))
+    newest_header = max(os.path.getmtime(h) for h in headers if os.path.exists(h))
+
     def compile_one(src):
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        # an object newer than its source and every header is up to date
+        if not force and os.path.exists(obj) and os.path.getmtime(obj) > max(os.path.getmtime(src), newest_header):
+            return src, obj, subprocess.CompletedProcess([], 0, "", "")
         cmd = [*common, "-c", "-o", obj, src]
         if src.endswith(".cpp"):
             cmd = [*common, "-x", "cu", "-c", "-o", obj, src]

@@ -18,15 +18,14 @@ namespace ddcb {
 
 namespace {
 
-// q (reference row order) from the kernel-order solution qk: q[(i + rrot) mod n] = qk[i], with the
-// rows of the Hermite derivatives scaled by dx^k (the derivative inputs are unscaled).
-__global__ void unrotate_scale_kernel(const double* __restrict__ qk, double* __restrict__ q, int n, int rrot,
-                                      int nbv_lo, int nbv_hi, double dx, int odd)
+// q from the solution qk of A^T qk = I (both in the reference's row order), with the rows of the
+// Hermite derivatives scaled by dx^k (the derivative inputs are unscaled).
+__global__ void scale_hermite_rows_kernel(const double* __restrict__ qk, double* __restrict__ q, int n, int nbv_lo,
+                                          int nbv_hi, double dx, int odd)
 {
-    int const i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int const r = (i + rrot) % n;
-    double v = qk[i];
+    int const r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    double v = qk[r];
     int e = -1;
     if (r < nbv_lo) e = r + odd;
     else if (r >= n - nbv_hi) e = r - (n - nbv_hi) + odd;
@@ -100,16 +99,17 @@ __global__ void __launch_bounds__(32 * S) integrate_samples_kernel(const __grid_
 
 void compute_device_quadrature(Builder& b, double* d_qk, double* d_q)
 {
-    // right-hand side in kernel order: column j of the rotated system is B-spline (j + crot) mod n
+    // right-hand side: the integrals of the first n B-splines in basis order (the periodic
+    // duplicates are not part of the system); the multi-right-hand-side solve takes and returns
+    // the reference's row / column order (it applies the kernel's rotations itself)
     long const n = b.n;
-    std::vector<double> ints(b.basis.size()), rk(n);
+    std::vector<double> ints(b.basis.size());
     basis_integrals(b.basis, ints.data());
-    for (long j = 0; j < n; ++j) rk[j] = ints[(j + b.crot) % n];
-    DDCB_CUDA_CHECK(cudaMemcpy(d_qk, rk.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    DDCB_CUDA_CHECK(cudaMemcpy(d_qk, ints.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
     cudaStream_t const s = nullptr;
     launch_solve_multirhs(b, d_qk, 1, 1, true, s);
-    unrotate_scale_kernel<<<dim3((unsigned)((n + 127) / 128)), dim3(128), 0, s>>>(d_qk, d_q, int(n), b.rrot, b.nbv_lo,
-                                                                              b.nbv_hi, b.dx, b.odd);
+    scale_hermite_rows_kernel<<<dim3((unsigned)((n + 127) / 128)), dim3(128), 0, s>>>(d_qk, d_q, int(n), b.nbv_lo, b.nbv_hi,
+                                                                                  b.dx, b.odd);
     DDCB_CUDA_CHECK(cudaGetLastError());
     DDCB_CUDA_CHECK(cudaStreamSynchronize(s));
 }

@@ -137,3 +137,28 @@ def test_refined_2d_build(D, oracle_mod):
     b2(coefs, cuda(vals), derivs_min2=cuda(dmin2), derivs_max2=cuda(dmax2))
     torch.cuda.synchronize()
     assert relerr(coefs.cpu().numpy(), ref) <= 1e-12
+
+
+@pytest.mark.parametrize("rounds", [1, 2])
+def test_config5_forward_full_size(D, oracle_mod, rounds):
+    """The differentiation workload's forward pass at its named size: periodic uniform cubic, 1024
+    cells, 65536 lines, FP32 solves with FP64 refinement, build then evaluation at 1024 random
+    points per line (the fused kernel, or the two kernels), against the oracle's FP64 build and
+    evaluation of the same inputs: <= 1e-12 (coefficients and values)."""
+    from tests.test_gpu_adjoint import config5_inputs
+
+    O = oracle_mod
+    B = 1 << 16
+    vals, coords, _ = config5_inputs(B)
+    bs = D.UniformBSplines(3, True, 0.0, 1.0, 1024)
+    obs = O.BSplines(3, True, rmin=0.0, rmax=1.0, ncells=1024)
+    pts = D.greville_points(bs, P, P)
+    ref = O.Builder(obs, pts, P, P)(vals)
+    want = O.evaluate(obs, coords, ref, ex_lo=0, ex_hi=0)
+    b = D.SplineBuilder(bs, None, P, P, precision="fp32_refine", refine_rounds=rounds)
+    e = D.SplineEvaluator(bs)
+    c = torch.empty((bs.size, B), dtype=torch.float64, device="cuda")
+    y = torch.empty((1024, B), dtype=torch.float64, device="cuda")
+    b.build_and_evaluate(e, c, cuda(vals), cuda(coords), y)
+    assert relerr(c.cpu().numpy(), ref) <= 1e-12
+    assert relerr(y.cpu().numpy(), want) <= 1e-12
