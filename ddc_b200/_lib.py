@@ -111,6 +111,8 @@ SIGNATURES = {
     "ddcb_integratend": [_vp, C.c_int32, _vp, _vp, C.c_int64, _vp],
     "ddcb_build_eval": [_vp, _vp, C.c_int32, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines,
                         C.POINTER(C.c_int32), _vp],
+    "ddcb_advect": [_vp, _vp, C.c_double, _vp, C.c_int64, C.c_double, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines,
+                    _vp, Lines, C.POINTER(C.c_int32), _vp],
     "ddcb_build_adjoint": [_vp, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp],
     "ddcb_eval_adjoint": [_vp, C.c_int32, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp],
     "ddcb_build_eval_adjoint": [_vp, _vp, C.c_int32, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp,

@@ -395,6 +395,38 @@ ddcb_status ddcb_build_eval(ddcb_builder h, ddcb_evaluator he, int32_t order, do
     });
 }
 
+ddcb_status ddcb_advect(ddcb_builder h, ddcb_evaluator he, double dt, const double* velocity, int64_t velocity_div,
+                        double velocity_const, double* out, ddcb_lines lo, const double* vals, ddcb_lines lv,
+                        const double* dlo, ddcb_lines llo, const double* dhi, ddcb_lines lhi, double* coefs, ddcb_lines lc,
+                        int32_t* fused, ddcb_stream stream)
+{
+    return guarded(__func__, [&] {
+        if (fused) *fused = 0;
+        require(h != nullptr && he != nullptr, "builder or evaluator is NULL");
+        ddcb::Builder const& b = *h->b;
+        ddcb::Evaluator const& e = *he->e;
+        require(e.basis.desc.degree == b.basis.desc.degree && e.basis.desc.ncells == b.basis.desc.ncells
+                    && e.basis.desc.uniform == b.basis.desc.uniform && e.basis.desc.periodic == b.basis.desc.periodic,
+                "builder and evaluator use different bases");
+        require(std::isfinite(dt) && std::isfinite(velocity_const), "dt and velocity_const must be finite");
+        // the coefficient output is optional: check it like ddcb_build when given
+        double* const c_req = coefs;
+        ddcb_lines const lc_req = coefs ? lc : ddcb_lines {b.basis.size(), lv.inner, lv.inner, lv.outer, lv.inner * b.basis.size()};
+        double dummy = 0.0;
+        if (!check_build(h, coefs ? coefs : &dummy, lc_req, vals, lv, dlo, llo, dhi, lhi)) return;
+        check_lines(lo, int64_t(b.points.size()), "out");
+        same_batch(lo, lv, "out/vals");
+        require(out != nullptr, "out is NULL");
+        int64_t const nl = lv.inner * lv.outer;
+        if (velocity) require(velocity_div >= 1, "velocity_div must be >= 1");
+        ddcb::Lines const lcl = ddcb::to_lines(lc_req);
+        bool const f = ddcb::launch_advect(b, e, dt, velocity, velocity_const, velocity ? velocity_div : nl, out,
+                                           ddcb::to_lines(lo), vals, ddcb::to_lines(lv), dlo, ddcb::to_lines(llo), dhi,
+                                           ddcb::to_lines(lhi), c_req, lcl, reinterpret_cast<cudaStream_t>(stream));
+        if (fused) *fused = f ? 1 : 0;
+    });
+}
+
 ddcb_status ddcb_build(ddcb_builder h, double* coefs, ddcb_lines lc, const double* vals, ddcb_lines lv,
                        const double* dlo, ddcb_lines llo, const double* dhi, ddcb_lines lhi, ddcb_stream stream)
 {

@@ -2,6 +2,7 @@
 // spline_builder.hpp:896-1101) as one kernel per call; the per-tile algorithm is in
 // build_device.cuh.
 #include <algorithm>
+#include <string>
 
 #include "build_device.cuh"
 
@@ -85,6 +86,8 @@ int pick_nct(SolveTables const& t, int TL)
 
 bool launch_build_eval_fused(BuildArgs const& args, Evaluator const& e, int order, double* out, Lines const& lo,
                              double const* coords, Lines const& lx, cudaStream_t s);
+bool launch_advect_fused(BuildArgs const& args, Evaluator const& e, double const* pts, double dt, double const* velocity,
+                         double v_const, int64_t v_div, double* out, Lines const& lo, cudaStream_t s);
 void launch_refine(BuildArgs const& args, int TL, int rounds, cudaStream_t s);
 
 namespace {
@@ -129,6 +132,55 @@ bool launch_build_eval(Builder const& b, Evaluator const& e, int order, double* 
         launch_eval(e, order, out, lo, coords, lx, coefs, lc, s);
     }
     return fused;
+}
+
+namespace {
+// feet[q * nl + b] = pts[q] - dt * v(b): the evaluation coordinates of the unfused advection step.
+__global__ void feet_kernel(double* __restrict__ feet, const double* __restrict__ pts, int64_t m, int64_t nl, double dt,
+                            const double* __restrict__ velocity, double v_const, int64_t v_div)
+{
+    int64_t const i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m * nl) return;
+    int64_t const q = i / nl, b = i % nl;
+    feet[i] = __ldg(pts + q) - dt * (velocity ? __ldg(velocity + b / v_div) : v_const);
+}
+} // namespace
+
+bool launch_advect(Builder const& b, Evaluator const& e, double dt, double const* velocity, double v_const, int64_t v_div,
+                   double* out, Lines const& lo, double const* vals, Lines const& lv, double const* dlo, Lines const& llo,
+                   double const* dhi, Lines const& lhi, double* coefs, Lines const& lc, cudaStream_t s)
+{
+    int64_t const nl = lv.nlines(), m = lo.n;
+    if (nl == 0 || m == 0) return true;
+    if (b.tile_lines == 8 && b.precision == DDCB_FP64) {
+        BuildArgs args = make_build_args(b, coefs, lc, vals, lv, dlo, llo, dhi, lhi);
+        args.nct = std::max(args.nct, 64);
+        if (launch_advect_fused(args, e, b.d_points, dt, velocity, v_const, v_div, out, lo, s)) return true;
+    }
+    // build, feet, evaluate: the coefficients and the feet in stream-ordered scratch
+    Lines const lscratch {int64_t(b.basis.size()), nl, nl, 1, 0};
+    double* c = coefs;
+    double* feet = nullptr;
+    if (c == nullptr) DDCB_CUDA_CHECK(cudaMallocAsync(reinterpret_cast<void**>(&c), sizeof(double) * size_t(b.basis.size() * nl), s));
+    cudaError_t const fe = cudaMallocAsync(reinterpret_cast<void**>(&feet), sizeof(double) * size_t(m * nl), s);
+    if (fe != cudaSuccess) {
+        if (coefs == nullptr) cudaFreeAsync(c, s);
+        throw Error(DDCB_ERR_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(fe));
+    }
+    try {
+        Lines const lcc = coefs ? lc : lscratch;
+        launch_build(b, c, lcc, vals, lv, dlo, llo, dhi, lhi, s);
+        feet_kernel<<<dim3((unsigned)((m * nl + 255) / 256)), dim3(256), 0, s>>>(feet, b.d_points, m, nl, dt, velocity, v_const, v_div);
+        DDCB_CUDA_CHECK(cudaGetLastError());
+        launch_eval(e, 0, out, lo, feet, Lines {m, nl, nl, 1, 0}, c, lcc, s);
+    } catch (...) {
+        cudaFreeAsync(feet, s);
+        if (coefs == nullptr) cudaFreeAsync(c, s);
+        throw;
+    }
+    DDCB_CUDA_CHECK(cudaFreeAsync(feet, s));
+    if (coefs == nullptr) DDCB_CUDA_CHECK(cudaFreeAsync(c, s));
+    return false;
 }
 
 void launch_build(Builder const& b, double* coefs, Lines const& lc, double const* vals, Lines const& lv,

@@ -164,7 +164,10 @@ struct Builder
     size_t d_block_bytes = 0;
     double* d_quad = nullptr;      // quadrature weights (n, reference row order, Hermite rows scaled
                                    // by dx^k), computed on the device at creation; inside d_block
-    double* d_quad_scratch = nullptr; // n doubles of d_block for that computation
+    double* d_quad_scratch = nullptr; // n doubles of d_block for that computation, then size() more
+    double* d_iweights = nullptr;  // integration weights of the interpolating spline: [values (npoints),
+                                   // lower derivatives (nbv_lo), upper derivatives (nbv_hi)]
+    double* d_points = nullptr;    // the interpolation points on the device (inside d_block)
     RhsMap rhs {};
     std::string structure;
     void* host_private = nullptr;  // host factorisation (plan.cpp)
@@ -215,6 +218,15 @@ void launch_solve_multirhs(Builder const& b, double* rhs, long ld, long nrhs, bo
 bool launch_build_eval(Builder const& b, Evaluator const& e, int order, double* coefs, Lines const& lc,
                        double const* vals, Lines const& lv, double const* dlo, Lines const& llo, double const* dhi,
                        Lines const& lhi, double const* coords, Lines const& lx, double* out, Lines const& lo, cudaStream_t s);
+
+// One semi-Lagrangian advection step (examples/characteristics_advection.cpp:243-259): build the
+// lines' splines, evaluate each at the feet pts[q] - dt * v(b) of the interpolation points, with
+// v(b) = velocity[b / v_div] or v_const. coefs may be NULL (not kept). Returns true when one
+// fused kernel ran (uniform bases); otherwise a build, a feet kernel and an evaluation run with
+// stream-ordered scratch.
+bool launch_advect(Builder const& b, Evaluator const& e, double dt, double const* velocity, double v_const, int64_t v_div,
+                   double* out, Lines const& lo, double const* vals, Lines const& lv, double const* dlo, Lines const& llo,
+                   double const* dhi, Lines const& lhi, double* coefs, Lines const& lc, cudaStream_t s);
 
 // adjoint_kernels.cu
 void launch_build_adjoint(Builder const& b, double const* gc, Lines const& lgc, double* gv, Lines const& lgv,

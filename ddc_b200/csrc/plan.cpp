@@ -1052,9 +1052,13 @@ void upload_builder(Builder* b)
     std::vector<size_t> offs_f, offs_a;
     b->tables = upload_tables(priv->fwd, blob, offs_f);
     b->tables_t = upload_tables(priv->adj, blob, offs_a);
-    // the quadrature weights and their scratch (2 n doubles) follow the tables
+    // the quadrature weights and their scratch (2 n doubles) follow the tables, then the
+    // interpolation points (the advection step's feet start from them)
     size_t const qoff = (blob.size() + 255) & ~size_t(255);
-    blob.resize(qoff + 2 * sizeof(double) * size_t(b->n), 0);
+    size_t const nw = size_t(b->basis.size()) + b->points.size() + size_t(b->nbv_lo + b->nbv_hi);
+    size_t const poff = qoff + sizeof(double) * (2 * size_t(b->n) + nw);
+    blob.resize(poff + sizeof(double) * b->points.size(), 0);
+    std::memcpy(blob.data() + poff, b->points.data(), sizeof(double) * b->points.size());
     DDCB_CUDA_CHECK(cudaMalloc(&b->d_block, blob.size()));
     DDCB_CUDA_CHECK(cudaMemcpy(b->d_block, blob.data(), blob.size(), cudaMemcpyHostToDevice));
     b->d_block_bytes = blob.size();
@@ -1062,6 +1066,8 @@ void upload_builder(Builder* b)
     bind_tables(b->tables_t, static_cast<char*>(b->d_block), offs_a.data());
     b->d_quad_scratch = reinterpret_cast<double*>(static_cast<char*>(b->d_block) + qoff);
     b->d_quad = b->d_quad_scratch + b->n;
+    b->d_iweights = b->d_quad + b->n + b->basis.size();
+    b->d_points = reinterpret_cast<double*>(static_cast<char*>(b->d_block) + poff);
 }
 
 Builder* create_builder(Basis const& basis, double const* pts, long npts, int lo, int hi, ddcb_builder_options const* opts)

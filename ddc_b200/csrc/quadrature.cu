@@ -5,10 +5,17 @@
 // the integral of B-spline j (integrals.hpp), so that the integral of the spline built from a
 // right-hand side f is I . A^-1 f = q . f. Here the transposed solve is the device kernel of the
 // multi-right-hand-side solve (in place, on one column), run once when the builder is created;
-// the weights stay on the device. integrate_samples then computes, per batch line, the integral
-// of the spline interpolating its samples (and Hermite derivatives) as one dot product: a single
-// read of the samples, with no coefficient array written or read -- the builder and
-// SplineEvaluator::integrate fused into one HBM pass.
+// the weights stay on the device.
+//
+// The reference takes I in basis order without the periodic column offset of the builder
+// (spline_builder.hpp:619-658, 1061-1100), so on non-uniform periodic bases with a non-zero offset
+// (degree >= 2), whose B-spline integrals differ, its q . f is not the integral of the spline the
+// builder returns. quadrature_coefficients keeps the reference's numbers. integrate_samples uses
+// the exact weights instead: the builder's adjoint applied to I (w = R^T A^-T P^T I, with the
+// offset, the periodic duplicates and the dx^k scaling of Hermite inputs), so that, per batch line,
+// w . (samples, derivatives) is the integral of the interpolating spline -- one read of the
+// samples, with no coefficient array written or read: the builder and SplineEvaluator::integrate
+// fused into one HBM pass.
 #include <algorithm>
 #include <vector>
 
@@ -39,10 +46,10 @@ __global__ void scale_hermite_rows_kernel(const double* __restrict__ qk, double*
 
 struct IntegrateArgs
 {
-    const double* q;     // n weights, reference row order, Hermite rows scaled by dx^k
-    int nbe_lo, npoints; // value k of a line pairs with q[nbe_lo + k] (nbe_lo = 0 when periodic)
-    int nbv_lo, nbv_hi;  // derivative k pairs with q[k] (lower) / q[n - nbe_hi + k] (upper)
-    int hi0;             // n - nbe_hi
+    const double* w;     // value k pairs with w[k], lower derivative k with w[npoints + k], upper
+    int npoints;         // derivative k with w[npoints + nbv_lo_all + k]
+    int nbv_lo, nbv_hi;  // derivative rows read (0 when the data are not given)
+    int nbv_lo_all;
     int64_t nlines;
     const double* vals;
     Lines lv;
@@ -67,7 +74,7 @@ __global__ void __launch_bounds__(32 * S) integrate_samples_kernel(const __grid_
     double acc = 0.0;
     if (line < a.nlines) {
         const double* v = a.vals + line_off(a.lv, line);
-        const double* q = a.q + a.nbe_lo;
+        const double* q = a.w;
         int r = s;
         // four independent partial sums keep several loads in flight
         double acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
@@ -80,9 +87,10 @@ __global__ void __launch_bounds__(32 * S) integrate_samples_kernel(const __grid_
         for (; r < a.npoints; r += S) acc = fma(__ldg(q + r), __ldcs(v + (int64_t)r * a.lv.stride), acc);
         acc += (acc1 + acc2) + acc3;
         if (s == 0) {
-            for (int k = 0; k < a.nbv_lo; ++k) acc = fma(__ldg(a.q + k), a.dlo[k * a.llo.stride + line_off(a.llo, line)], acc);
-            for (int k = 0; k < a.nbv_hi; ++k)
-                acc = fma(__ldg(a.q + a.hi0 + k), a.dhi[k * a.lhi.stride + line_off(a.lhi, line)], acc);
+            const double* wd = a.w + a.npoints;
+            for (int k = 0; k < a.nbv_lo; ++k) acc = fma(__ldg(wd + k), a.dlo[k * a.llo.stride + line_off(a.llo, line)], acc);
+            wd += a.nbv_lo_all;
+            for (int k = 0; k < a.nbv_hi; ++k) acc = fma(__ldg(wd + k), a.dhi[k * a.lhi.stride + line_off(a.lhi, line)], acc);
         }
     }
     part[s][l] = acc;
@@ -111,6 +119,17 @@ void compute_device_quadrature(Builder& b, double* d_qk, double* d_q)
     scale_hermite_rows_kernel<<<dim3((unsigned)((n + 127) / 128)), dim3(128), 0, s>>>(d_qk, d_q, int(n), b.nbv_lo, b.nbv_hi,
                                                                                   b.dx, b.odd);
     DDCB_CUDA_CHECK(cudaGetLastError());
+    // the exact integration weights: the builder adjoint of the integrals of all size() B-splines
+    // (one line; the integrals follow q in the block, the weights follow them)
+    long const sz = b.basis.size();
+    double* const d_ints = d_q + n;
+    DDCB_CUDA_CHECK(cudaMemcpy(d_ints, ints.data(), sizeof(double) * sz, cudaMemcpyHostToDevice));
+    long const np = long(b.points.size());
+    bool const hlo = b.lo == DDCB_HERMITE && b.nbv_lo > 0, hhi = b.hi == DDCB_HERMITE && b.nbv_hi > 0;
+    Lines const none {0, 1, 0, 0, 0};
+    launch_build_adjoint(b, d_ints, Lines {sz, 1, 1, 1, 0}, b.d_iweights, Lines {np, 1, 1, 1, 0},
+                         hlo ? b.d_iweights + np : nullptr, hlo ? Lines {b.nbv_lo, 1, 1, 1, 0} : none,
+                         hhi ? b.d_iweights + np + b.nbv_lo : nullptr, hhi ? Lines {b.nbv_hi, 1, 1, 1, 0} : none, s);
     DDCB_CUDA_CHECK(cudaStreamSynchronize(s));
 }
 
@@ -118,12 +137,11 @@ void launch_integrate_samples(Builder const& b, double* out, int64_t out_outer_s
                               double const* dlo, Lines const& llo, double const* dhi, Lines const& lhi, cudaStream_t s)
 {
     IntegrateArgs a {};
-    a.q = b.d_quad;
-    a.nbe_lo = b.rhs.periodic ? 0 : b.nbe_lo;
+    a.w = b.d_iweights;
     a.npoints = int(b.points.size());
     a.nbv_lo = dlo ? b.nbv_lo : 0;
     a.nbv_hi = dhi ? b.nbv_hi : 0;
-    a.hi0 = int(b.n) - b.nbe_hi;
+    a.nbv_lo_all = (b.lo == DDCB_HERMITE) ? b.nbv_lo : 0;
     a.nlines = lv.nlines();
     a.vals = vals;
     a.lv = lv;

@@ -230,6 +230,34 @@ class SplineBuilder:
                   lines_of(out, dim), C.byref(fused), _stream_handle(stream))
         return bool(fused.value)
 
+    def advect(self, evaluator: "SplineEvaluator", f_out, f_in, dt: float, velocity=0.0, derivs_xmin=None,
+               derivs_xmax=None, spline=None, *, velocity_div: int = 1, dim: int = 0, stream=None) -> bool:
+        """One semi-Lagrangian advection step (examples/characteristics_advection.cpp:243-259): the
+        spline of every line of f_in evaluated at the feet x_q - dt * v of the interpolation points,
+        into f_out. velocity: a float (every line) or a CUDA float64 tensor, line b taking
+        velocity[b // velocity_div] (batch lines in the layout's order). spline, when given, receives
+        the coefficients. Returns True when one fused kernel did the step."""
+        out = _dev_f64(f_out, "f_out")
+        vals = _dev_f64(f_in, "f_in")
+        dlo = _dev_f64(derivs_xmin, "derivs_xmin")
+        dhi = _dev_f64(derivs_xmax, "derivs_xmax")
+        c = _dev_f64(spline, "spline")
+        vt = None
+        vconst = 0.0
+        if isinstance(velocity, (int, float)):
+            vconst = float(velocity)
+        else:
+            vt = _dev_f64(velocity, "velocity")
+            assert vt.is_contiguous()
+        empty = Lines(0, 1, 0, 0, 0)
+        fused = C.c_int32(0)
+        _lib.call("ddcb_advect", self._h, evaluator._h, float(dt), _ptr(vt), int(velocity_div), vconst, _ptr(out),
+                  lines_of(out, dim), _ptr(vals), lines_of(vals, dim), _ptr(dlo),
+                  lines_of(dlo, dim) if dlo is not None else empty, _ptr(dhi),
+                  lines_of(dhi, dim) if dhi is not None else empty, _ptr(c), lines_of(c, dim) if c is not None else empty,
+                  C.byref(fused), _stream_handle(stream))
+        return bool(fused.value)
+
     def adjoint(self, g_spline, g_vals, g_derivs_xmin=None, g_derivs_xmax=None, *, dim: int = 0, stream=None):
         """Reverse mode of operator(): given the cotangents g_spline of the coefficients, writes the
         cotangents of vals (and of the Hermite derivatives, when tensors are given) -- the transposed

@@ -181,6 +181,21 @@ ddcb_status ddcb_build_eval(ddcb_builder b, ddcb_evaluator e, int32_t order, dou
                             const double* coords, ddcb_lines coords_layout, double* out, ddcb_lines out_layout,
                             int32_t* fused, ddcb_stream stream);
 
+/* ---- one semi-Lagrangian advection step (examples/characteristics_advection.cpp:243-259): the
+ *      feet of the characteristics through the interpolation points, x_q - dt * v, the splines of
+ *      the lines (SplineBuilder::operator()) and their values at the feet (SplineEvaluator::operator(),
+ *      with the evaluator's periodic wrap or extrapolation rules), written to out at the
+ *      interpolation points (out's n is the builder's npoints). The velocity of line b is
+ *      velocity[b / velocity_div] (a device array; velocity_div = 1: one value per line, inner:
+ *      one per group of inner lines), or velocity_const when velocity is NULL. coefs (may be NULL)
+ *      receives the coefficients. On uniform bases one kernel does the whole step and the feet are
+ *      computed in it (no coordinate array is read); *fused (may be NULL) tells whether it ran. - */
+ddcb_status ddcb_advect(ddcb_builder b, ddcb_evaluator e, double dt, const double* velocity, int64_t velocity_div,
+                        double velocity_const, double* out, ddcb_lines out_layout, const double* vals,
+                        ddcb_lines vals_layout, const double* derivs_lo, ddcb_lines derivs_lo_layout,
+                        const double* derivs_hi, ddcb_lines derivs_hi_layout, double* coefs, ddcb_lines coefs_layout,
+                        int32_t* fused, ddcb_stream stream);
+
 /* ---- reverse mode (no reference counterpart: the reference has no derivatives with respect to
  *      its inputs). The builder is linear, coefs = P A^-1 R (vals, dx^k derivs); the evaluator is
  *      y = sum_i c[jmin+i] B_i(x). Every cotangent output is overwritten, not accumulated. ---- */

@@ -38,7 +38,9 @@ struct Rank<Q, TypeSeq<>>
 template <class Q, class H, class... T>
 struct Rank<Q, TypeSeq<H, T...>>
 {
-    static constexpr std::size_t value = std::is_same_v<Q, H> ? 0 : 1 + Rank<Q, TypeSeq<T...>>::value;
+    static constexpr std::size_t rest = Rank<Q, TypeSeq<T...>>::value;
+    static constexpr std::size_t value
+            = std::is_same_v<Q, H> ? 0 : (rest == std::numeric_limits<std::size_t>::max() ? rest : 1 + rest);
 };
 } // namespace detail
 
