@@ -49,7 +49,7 @@ class BSplinesInfo(C.Structure):
 
 class BuilderOptions(C.Structure):
     _fields_ = [("precision", C.c_int32), ("refine_rounds", C.c_int32), ("tile_lines", C.c_int32),
-                ("chunks", C.c_int32)]
+                ("chunks", C.c_int32), ("refine_tolerance", C.c_double)]
 
 
 class BuilderInfo(C.Structure):
@@ -82,6 +82,7 @@ SIGNATURES = {
     "ddcb_builder_create": [_vp, _vp, C.c_int64, C.c_int, C.c_int, C.POINTER(BuilderOptions), _pp],
     "ddcb_builder_destroy": [_vp],
     "ddcb_builder_get_info": [_vp, C.POINTER(BuilderInfo)],
+    "ddcb_builder_device_status": [_vp, _vp],
     "ddcb_build": [_vp, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp],
     "ddcb_solve_multirhs": [_vp, _vp, C.c_int64, C.c_int64, C.c_int32, _vp],
     "ddcb_quadrature_coefficients": [_vp, _vp, _vp, _vp],

@@ -588,7 +588,7 @@ void launch_build_adjoint(Builder const& b, double const* gc, Lines const& lgc, 
 {
     AdjointArgs a = make_adjoint_args(b, gc, lgc, gv, lgv, gdlo, lglo, gdhi, lghi);
     if (a.nlines == 0) return;
-    int const TL = fit_tile_lines(b.tile_lines, [&](int w) { return sizeof(double) * tile_doubles(a.t, w, a.t.kl, a.t.ku); });
+    int const TL = fit_tile_lines(std::min(b.tile_lines, 8), [&](int w) { return sizeof(double) * tile_doubles(a.t, w, a.t.kl, a.t.ku); });
     a.nct = adj_nct(a.t, TL, 128);
     dispatch_build_adjoint(a, TL, s);
 }

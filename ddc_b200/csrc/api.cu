@@ -2,6 +2,7 @@
 // runs the C++ plan / kernel code and turns every C++ exception into a ddcb_status.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -299,6 +300,31 @@ ddcb_status ddcb_builder_create(ddcb_bsplines basis, const double* interp_points
     });
 }
 
+static void check_device(int device, char const* what);
+
+ddcb_status ddcb_builder_device_status(ddcb_builder h, ddcb_stream stream)
+{
+    ddcb_status st = DDCB_SUCCESS;
+    ddcb_status const g = guarded(__func__, [&] {
+        require(h != nullptr, "builder is NULL");
+        ddcb::Builder const& b = *h->b;
+        check_device(b.device, "builder");
+        cudaStream_t const s = reinterpret_cast<cudaStream_t>(stream);
+        unsigned word = 0;
+        DDCB_CUDA_CHECK(cudaMemcpyAsync(&word, b.d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        DDCB_CUDA_CHECK(cudaStreamSynchronize(s));
+        if (word != 0) {
+            DDCB_CUDA_CHECK(cudaMemsetAsync(b.d_status, 0, sizeof(unsigned), s));
+            DDCB_CUDA_CHECK(cudaStreamSynchronize(s));
+            char msg[160];
+            std::snprintf(msg, sizeof msg, "a refined FP32 solve ended with an estimated relative error above %.3g",
+                          b.refine_tolerance);
+            throw ddcb::Error(DDCB_ERR_NOT_CONVERGED, msg);
+        }
+    });
+    return g != DDCB_SUCCESS ? g : st;
+}
+
 ddcb_status ddcb_builder_destroy(ddcb_builder b)
 {
     return guarded(__func__, [&] {
@@ -449,8 +475,6 @@ ddcb_status ddcb_solve_multirhs(ddcb_builder h, double* rhs, int64_t ld, int64_t
         ddcb::launch_solve_multirhs(*h->b, rhs, long(ld), long(nrhs), transpose != 0, reinterpret_cast<cudaStream_t>(stream));
     });
 }
-
-static void check_device(int device, char const* what);
 
 ddcb_status ddcb_quadrature_coefficients(ddcb_builder h, double* qlo, double* q, double* qhi)
 {

@@ -12,12 +12,13 @@ namespace {
 
 // MAXT: the largest block the instantiation takes. Blocks of up to 256 threads (64 chunks of
 // 8-line tiles, the default) get up to 128 registers, which lets the sweeps of narrow bands
-// unroll 8 rows and keep more factor loads in flight; larger blocks keep 64 registers.
+// unroll 8 rows and keep more factor loads in flight; so do the 512-thread blocks of 16-line
+// tiles (one per SM); other large blocks keep 64 registers.
 template <int TL, int KL, int KU, int MAXT>
 __global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 2 : 1) build_kernel(const __grid_constant__ BuildArgs args)
 {
     extern __shared__ __align__(16) double smem[];
-    solve_tile<TL, KL, KU, (MAXT <= 256 && TL >= 4 && KL + KU <= 6) ? 8 : 0>(args, smem);
+    solve_tile<TL, KL, KU, (MAXT <= 512 && TL >= 4 && KL + KU <= 6) ? 8 : 0>(args, smem);
     store_tile<TL>(args, smem);
 }
 
@@ -34,7 +35,9 @@ void launch_tl(BuildArgs const& args, cudaStream_t s)
     if (sm > size_t(optin))
         throw Error(DDCB_ERR_UNSUPPORTED, "line tile of " + std::to_string(sm) + " bytes exceeds shared memory (" + std::to_string(optin)
                                               + "); use fewer tile lines");
-    auto kern = TL * nct <= 256 ? build_kernel<TL, KL, KU, 256> : build_kernel<TL, KL, KU, 1024>;
+    auto kern = TL == 16 ? build_kernel<TL, KL, KU, 512>
+                         : (TL * nct <= 256 ? build_kernel<TL, KL, KU, 256> : build_kernel<TL, KL, KU, 1024>);
+    if (TL == 16 && TL * nct > 512) throw Error(DDCB_ERR_UNSUPPORTED, "16-line tiles take at most 32 chunk threads per line");
     if (sm > 48 * 1024) DDCB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
     int64_t const grid = (args.nlines + TL - 1) / TL;
     kern<<<dim3((unsigned)grid), dim3(TL * nct), sm, s>>>(args);
@@ -48,7 +51,8 @@ void launch_k(BuildArgs const& args, int TL, cudaStream_t s)
     case 2: launch_tl<2, KL, KU>(args, s); break;
     case 4: launch_tl<4, KL, KU>(args, s); break;
     case 8: launch_tl<8, KL, KU>(args, s); break;
-    default: throw Error(DDCB_ERR_UNSUPPORTED, "tile_lines must be 2, 4 or 8");
+    case 16: launch_tl<16, KL, KU>(args, s); break;
+    default: throw Error(DDCB_ERR_UNSUPPORTED, "tile_lines must be 2, 4, 8 or 16");
     }
 }
 
@@ -208,7 +212,7 @@ void launch_build(Builder const& b, double* coefs, Lines const& lc, double const
     int const kl = b.tables.kl, ku = b.tables.ku;
     int TL;
     if (b.precision == DDCB_FP32_REFINE)
-        TL = fit_tile_lines(b.tile_lines, [&](int w) {
+        TL = fit_tile_lines(std::min(b.tile_lines, 8), [&](int w) {
             return sizeof(double) * (size_t)b.tables.n * w + sizeof(float) * tile_doubles(b.tables, w, kl, ku) + 16;
         });
     else

@@ -87,6 +87,12 @@ struct SolveTables
     const int* a_row;    // n+1
     const int* a_col;
     const double* a_val;
+    // refinement checks: an estimate of cond_inf(A) = ||A||_inf ||A^-1||_inf (Higham's 1-norm
+    // estimator for the inverse, on the host) and the builder's device status word (bit 0: a
+    // refined solve missed its bound)
+    double cond_est;
+    double refine_tol;
+    unsigned* status;
 };
 
 // Where the factor entries of row j live in the uploaded tables. Row-major tables (il = 0) store a
@@ -151,6 +157,7 @@ struct Builder
     std::vector<double> A;  // assembled dense matrix (n x n), kept for the adjoint / checks
     int precision = DDCB_FP64;
     int refine_rounds = 2;
+    double refine_tolerance = 1e-12; // bound on ||A^-1|| |b - A x| / |x| after the last round
     int device = -1;
     int tile_lines = 8;     // lines per CTA
     int nchunk_req = 64;    // requested chunks per line (64: fastest on 1000-row lines, large and small batches)
@@ -168,6 +175,8 @@ struct Builder
     double* d_iweights = nullptr;  // integration weights of the interpolating spline: [values (npoints),
                                    // lower derivatives (nbv_lo), upper derivatives (nbv_hi)]
     double* d_points = nullptr;    // the interpolation points on the device (inside d_block)
+    unsigned* d_status = nullptr;  // device status word (inside d_block): bit 0 = not converged
+    double cond_est = 0.0;         // estimate of ||A^-1||_inf
     RhsMap rhs {};
     std::string structure;
     void* host_private = nullptr;  // host factorisation (plan.cpp)

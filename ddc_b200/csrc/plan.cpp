@@ -927,6 +927,37 @@ struct BuilderPrivate
     SparseRows ref_rows; // the assembled system in the reference's row / column order
 };
 
+// An estimate of ||A^-1||_inf = ||A^-T||_1 by Higham's 1-norm estimator (N. J. Higham, ACM TOMS 14
+// (1988) 381-396, after Hager 1984): a few solves with A^T and A on sign vectors. It bounds the
+// forward error of a refined solution from its residual: |x - x*| <= ||A^-1|| |b - A x|.
+static double inverse_norm_estimate(HostSolve const& h)
+{
+    long const n = h.n;
+    if (n == 0) return 0.0;
+    std::vector<double> x(n, 1.0 / double(n)), y(n), z(n);
+    double est = 0.0;
+    for (int it = 0; it < 5; ++it) {
+        y = x;
+        h.solve_host(y.data(), true); // y = A^-T x
+        double e = 0.0;
+        for (double v : y) e += std::fabs(v);
+        if (it > 0 && e <= est) break;
+        est = e;
+        for (long i = 0; i < n; ++i) z[i] = y[i] >= 0.0 ? 1.0 : -1.0;
+        h.solve_host(z.data(), false); // z = A^-1 sign(y)
+        long j = 0;
+        double zx = 0.0;
+        for (long i = 0; i < n; ++i) {
+            zx += z[i] * x[i];
+            if (std::fabs(z[i]) > std::fabs(z[j])) j = i;
+        }
+        if (it > 0 && std::fabs(z[j]) <= zx) break;
+        std::fill(x.begin(), x.end(), 0.0);
+        x[j] = 1.0;
+    }
+    return est;
+}
+
 Builder* create_builder_host(Basis const& basis, double const* pts, long npts, int lo, int hi, ddcb_builder_options const* opts)
 {
     if (pts == nullptr && npts > 0) throw Error(DDCB_ERR_INVALID_ARGUMENT, "interpolation points pointer is NULL");
@@ -955,12 +986,16 @@ Builder* create_builder_host(Basis const& basis, double const* pts, long npts, i
             if (opts->precision != DDCB_FP64 && opts->precision != DDCB_FP32_REFINE)
                 throw Error(DDCB_ERR_INVALID_ARGUMENT, "unknown precision");
             b->precision = opts->precision;
-            if (opts->refine_rounds > 0) b->refine_rounds = std::min(opts->refine_rounds, 3);
+            if (opts->refine_rounds < 0 || opts->refine_rounds > 3)
+                throw Error(DDCB_ERR_INVALID_ARGUMENT, "refine_rounds must be in 0..3 (0: the default, 2)");
+            if (opts->refine_rounds > 0) b->refine_rounds = opts->refine_rounds;
+            if (!(opts->refine_tolerance >= 0.0)) throw Error(DDCB_ERR_INVALID_ARGUMENT, "refine_tolerance must be >= 0");
+            if (opts->refine_tolerance > 0.0) b->refine_tolerance = opts->refine_tolerance;
             if (opts->tile_lines > 0) b->tile_lines = opts->tile_lines;
             if (opts->chunks > 0) b->nchunk_req = opts->chunks;
         }
-        if (b->tile_lines != 2 && b->tile_lines != 4 && b->tile_lines != 8)
-            throw Error(DDCB_ERR_INVALID_ARGUMENT, "tile_lines must be 2, 4 or 8");
+        if (b->tile_lines != 2 && b->tile_lines != 4 && b->tile_lines != 8 && b->tile_lines != 16)
+            throw Error(DDCB_ERR_INVALID_ARGUMENT, "tile_lines must be 2, 4, 8 or 16");
         if (b->nchunk_req * b->tile_lines > 1024) throw Error(DDCB_ERR_INVALID_ARGUMENT, "tile_lines*chunks must be <= 1024");
         check_valid_grid(*b);
         // compute_offset (spline_builder.hpp:619-658)
@@ -1011,6 +1046,16 @@ Builder* create_builder_host(Basis const& basis, double const* pts, long npts, i
         b->ku = int(priv->fwd.ku);
         b->pivot = priv->fwd.pivot ? 1 : 0;
         b->structure = describe(priv->fwd);
+        {
+            // cond_inf(A) = ||A||_inf ||A^-1||_inf, the factor of the refinement's error bound
+            double anorm = 0.0;
+            for (auto const& row : priv->ref_rows) {
+                double s = 0.0;
+                for (auto const& [j, v] : row) s += std::fabs(v);
+                anorm = std::max(anorm, s);
+            }
+            b->cond_est = anorm * inverse_norm_estimate(priv->fwd);
+        }
         if (std::getenv("DDCB_DEBUG_PLAN")) {
             std::fprintf(stderr, "ddcb plan: %s | adjoint %s\n", b->structure.c_str(), describe(priv->adj).c_str());
             std::fprintf(stderr, "  swaps at:");
@@ -1057,7 +1102,8 @@ void upload_builder(Builder* b)
     size_t const qoff = (blob.size() + 255) & ~size_t(255);
     size_t const nw = size_t(b->basis.size()) + b->points.size() + size_t(b->nbv_lo + b->nbv_hi);
     size_t const poff = qoff + sizeof(double) * (2 * size_t(b->n) + nw);
-    blob.resize(poff + sizeof(double) * b->points.size(), 0);
+    size_t const soff = poff + sizeof(double) * b->points.size();
+    blob.resize(soff + 8, 0);
     std::memcpy(blob.data() + poff, b->points.data(), sizeof(double) * b->points.size());
     DDCB_CUDA_CHECK(cudaMalloc(&b->d_block, blob.size()));
     DDCB_CUDA_CHECK(cudaMemcpy(b->d_block, blob.data(), blob.size(), cudaMemcpyHostToDevice));
@@ -1068,6 +1114,10 @@ void upload_builder(Builder* b)
     b->d_quad = b->d_quad_scratch + b->n;
     b->d_iweights = b->d_quad + b->n + b->basis.size();
     b->d_points = reinterpret_cast<double*>(static_cast<char*>(b->d_block) + poff);
+    b->d_status = reinterpret_cast<unsigned*>(static_cast<char*>(b->d_block) + soff);
+    b->tables.cond_est = b->tables_t.cond_est = b->cond_est;
+    b->tables.refine_tol = b->tables_t.refine_tol = b->refine_tolerance;
+    b->tables.status = b->tables_t.status = b->d_status;
 }
 
 Builder* create_builder(Basis const& basis, double const* pts, long npts, int lo, int hi, ddcb_builder_options const* opts)

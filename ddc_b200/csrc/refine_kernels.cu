@@ -38,8 +38,35 @@ __device__ __forceinline__ void residual_tile(BuildArgs const& args, const doubl
     __syncthreads();
 }
 
-template <int TL, int KL, int KU>
-__global__ void __launch_bounds__(1024) refine_kernel(const __grid_constant__ BuildArgs args, int rounds)
+// The convergence check of the refined lines, from the last correction d (no extra residual
+// pass): the solve that produced d works in FP32 on an FP32-rounded residual, so the refined X
+// carries an error of about cond(A) (2^-24 max|d| + 2^-52 max|X|); a line whose bound, with a
+// factor 4, exceeds refine_tol * max|X| sets bit 0 of the builder's status word (read by
+// ddcb_builder_device_status). dmax / xmax: this thread's maxima of its line (threads own one line
+// each in the accumulation loops); `red`: 2 TL shared 8-byte words. Ends with a barrier.
+template <int TL>
+__device__ __forceinline__ void convergence_check(BuildArgs const& args, double dmax, double xmax, unsigned long long* red)
+{
+    SolveTables const& t = args.t;
+    int const l = threadIdx.x % TL;
+    if (threadIdx.x < 2 * TL) red[threadIdx.x] = 0ull;
+    __syncthreads();
+    // non-negative doubles order like their bit patterns
+    atomicMax(red + l, static_cast<unsigned long long>(__double_as_longlong(dmax)));
+    atomicMax(red + TL + l, static_cast<unsigned long long>(__double_as_longlong(xmax)));
+    __syncthreads();
+    if (threadIdx.x < TL && tile_line0<TL>(args) + threadIdx.x < args.nlines) {
+        double const d = __longlong_as_double(static_cast<long long>(red[threadIdx.x]));
+        double const x = __longlong_as_double(static_cast<long long>(red[TL + threadIdx.x]));
+        double const bound = 4.0 * t.cond_est * (0x1p-24 * d + 0x1p-52 * x);
+        if (!(bound <= t.refine_tol * x)) atomicOr(t.status, 1u);
+    }
+    __syncthreads();
+}
+
+// MAXT: the largest block the instantiation takes (blocks of up to 256 threads get 128 registers).
+template <int TL, int KL, int KU, int MAXT>
+__global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 2 : 1) refine_kernel(const __grid_constant__ BuildArgs args, int rounds)
 {
     extern __shared__ __align__(16) double smem[];
     int const n = args.t.n;
@@ -49,14 +76,27 @@ __global__ void __launch_bounds__(1024) refine_kernel(const __grid_constant__ Bu
     for (int i = threadIdx.x; i < n * TL; i += blockDim.x) W[i] = float(X[i]);
     __syncthreads();
     solve_in_tile<TL, KL, KU, float>(args.t, args.nct, W);
-    for (int i = threadIdx.x; i < n * TL; i += blockDim.x) X[i] = double(W[i]);
+    // every thread touches one line's elements (the block is a multiple of TL threads)
+    double dmax = 0.0, xmax = 0.0;
+    for (int i = threadIdx.x; i < n * TL; i += blockDim.x) {
+        X[i] = double(W[i]);
+        dmax = fmax(dmax, fabs(X[i]));
+    }
     __syncthreads();
     for (int round = 0; round < rounds; ++round) {
         residual_tile<TL>(args, X, W);
         solve_in_tile<TL, KL, KU, float>(args.t, args.nct, W);
-        for (int i = threadIdx.x; i < n * TL; i += blockDim.x) X[i] += double(W[i]);
+        dmax = 0.0;
+        for (int i = threadIdx.x; i < n * TL; i += blockDim.x) {
+            double const d = double(W[i]);
+            X[i] += d;
+            dmax = fmax(dmax, fabs(d));
+        }
         __syncthreads();
     }
+    for (int i = threadIdx.x; i < n * TL; i += blockDim.x) xmax = fmax(xmax, fabs(X[i]));
+    // the FP32 tile is free again: its first words hold the per-line maxima of the check
+    convergence_check<TL>(args, dmax, xmax, reinterpret_cast<unsigned long long*>(W));
     store_tile<TL>(args, X);
 }
 
@@ -75,7 +115,7 @@ void launch_refine_tl(BuildArgs const& args, int rounds, cudaStream_t s)
     DDCB_CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     if (sm > size_t(optin))
         throw Error(DDCB_ERR_UNSUPPORTED, "refinement tile of " + std::to_string(sm) + " bytes exceeds shared memory; use fewer tile lines");
-    auto kern = refine_kernel<TL, KL, KU>;
+    auto kern = TL * args.nct <= 256 ? refine_kernel<TL, KL, KU, 256> : refine_kernel<TL, KL, KU, 1024>;
     if (sm > 48 * 1024) DDCB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
     int64_t const grid = (args.nlines + TL - 1) / TL;
     kern<<<dim3((unsigned)grid), dim3(TL * args.nct), sm, s>>>(args, rounds);

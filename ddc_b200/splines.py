@@ -163,7 +163,7 @@ class SplineBuilder:
 
     def __init__(self, bsplines: BSplines, interpolation_points: Optional[Sequence[float]] = None,
                  lower: int = GREVILLE, upper: int = GREVILLE, *, precision: str = "fp64", refine_rounds: int = 2,
-                 tile_lines: int = 0, chunks: int = 0):
+                 tile_lines: int = 0, chunks: int = 0, refine_tolerance: float = 0.0):
         if bsplines.periodic:
             lower = upper = PERIODIC
         self.bsplines = bsplines
@@ -173,7 +173,7 @@ class SplineBuilder:
         pts = np.ascontiguousarray(interpolation_points, dtype=np.float64)
         self.interpolation_points = pts
         opts = BuilderOptions(FP32_REFINE if precision == "fp32_refine" else FP64, int(refine_rounds),
-                              int(tile_lines), int(chunks))
+                              int(tile_lines), int(chunks), float(refine_tolerance))
         h = C.c_void_p()
         _lib.call("ddcb_builder_create", bsplines._h, pts.ctypes.data_as(C.c_void_p), pts.size, int(lower),
                   int(upper), C.byref(opts), C.byref(h))
@@ -197,6 +197,11 @@ class SplineBuilder:
     @property
     def npoints(self):
         return self.info.npoints
+
+    def device_status(self, stream=None):
+        """Raise DdcbError(DDCB_ERR_NOT_CONVERGED) if a refined solve queued so far missed its
+        bound (ddcb_builder_device_status: waits for the stream, clears the flag)."""
+        _lib.call("ddcb_builder_device_status", self._h, _stream_handle(stream))
 
     def __call__(self, spline, vals, derivs_xmin=None, derivs_xmax=None, *, dim: int = 0, stream=None):
         """SplineBuilder::operator()(spline, vals, derivs_xmin, derivs_xmax) (spline_builder.hpp:896-1101)."""

@@ -339,7 +339,7 @@ public:
         : m_interpolation_domain(interpolation_domain), m_label(std::move(label))
     {
         std::vector<double> const pts = ddc_b200::interpolation_points_of(interpolation_domain);
-        ddcb_builder_options opts {DDCB_FP64, 2, 0, 0};
+        ddcb_builder_options opts {DDCB_FP64, 2, 0, 0, 0.0};
         ddcb_status const s = ddcb_builder_create(m_basis.get(), pts.data(), int64_t(pts.size()), ddc_b200::closure_of(SBCLower),
                                                   ddc_b200::closure_of(SBCUpper), &opts, &m_b);
         ddc_b200::check(s);

@@ -81,10 +81,13 @@ typedef struct ddcb_bsplines_info {
 } ddcb_bsplines_info;
 
 typedef struct ddcb_builder_options {
-    int32_t precision;     /* ddcb_precision */
-    int32_t refine_rounds; /* FP32_REFINE: refinement rounds (1..3) */
-    int32_t tile_lines;    /* 0 = automatic: lines per thread block */
-    int32_t chunks;        /* 0 = automatic: chunk threads per line */
+    int32_t precision;       /* ddcb_precision */
+    int32_t refine_rounds;   /* FP32_REFINE: refinement rounds (1..3; 0 = 2) */
+    int32_t tile_lines;      /* 0 = automatic: lines per thread block */
+    int32_t chunks;          /* 0 = automatic: chunk threads per line */
+    double refine_tolerance; /* FP32_REFINE: bound on the estimated relative error of a refined line,
+                                ||A^-1||_inf max|b - A x| / max|x| after the last round, checked on
+                                the device (0 = 1e-12); see ddcb_builder_device_status */
 } ddcb_builder_options;
 
 typedef struct ddcb_builder_info {
@@ -124,6 +127,11 @@ ddcb_status ddcb_builder_create(ddcb_bsplines basis, const double* interp_points
                                 ddcb_builder* out);
 ddcb_status ddcb_builder_destroy(ddcb_builder b);
 ddcb_status ddcb_builder_get_info(ddcb_builder b, ddcb_builder_info* info);
+/* The outcome of the device-side checks of this builder's work queued so far on `stream`: waits for
+ * the stream, returns DDCB_ERR_NOT_CONVERGED if a FP32_REFINE solve ended above refine_tolerance
+ * since the previous query (the reference reports non-convergence of its iterative solver,
+ * splines_linear_problem_sparse.cpp:272-275), else DDCB_SUCCESS; the flag is then cleared. */
+ddcb_status ddcb_builder_device_status(ddcb_builder b, ddcb_stream stream);
 /* SplineBuilder::operator()(spline, vals, derivs_xmin, derivs_xmax) (spline_builder.hpp:538-557,
  * 896-1101). derivs_* are ignored (may be NULL) unless the closure is HERMITE; their layout's n is
  * s_nbv (derivative orders odd..odd+nbv-1, unscaled). */
