@@ -299,6 +299,15 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def _converged(builder):
+    """Whether the refined solves queued so far met the builder's bound (ddcb_builder_device_status)."""
+    try:
+        builder.device_status()
+        return True
+    except Exception:
+        return False
+
+
 def _time_ms(fn, reps, rotate=1):
     """Mean CUDA-event time of fn(i) over `reps` calls after 3 warm-ups; i cycles over `rotate`
     buffer sets (several sets larger than L2 in all keep each call's inputs out of L2)."""
@@ -365,9 +374,15 @@ def measure_configs(peak, reps):
         c = torch.empty_like(ref)
         t = _time_ms(lambda i: br_(c, v, lo, hi), reps)
         err = float((c - ref).abs().max() / ref.abs().max())
-        prec[f"fp32_refine_{rounds}_rounds"] = {"build_ms": t, "speedup_vs_fp64": t64 / t, "max_rel_err_vs_fp64": err}
+        prec[f"fp32_refine_{rounds}_rounds"] = {"build_ms": t, "speedup_vs_fp64": t64 / t, "max_rel_err_vs_fp64": err,
+                                                "converged": _converged(br_)}
     out["quintic_hermite_precision"] = prec
-    del v, lo, hi, ref
+    # ---- the same lines integrated straight from the samples (build + integrate in one pass) ----
+    integ = torch.empty(1 << 16, dtype=torch.float64, device=dev)
+    ti = _time_ms(lambda i: b64.integrate_samples(integ, v, lo, hi), 10 * reps)
+    ib = (v.numel() + lo.numel() + hi.numel() + integ.numel()) * 8
+    out["quintic_hermite_integrate_samples"] = {"ms": ti, "GBps": ib / ti / 1e6, "hbm_frac": ib / ti / 1e6 / peak}
+    del v, lo, hi, ref, integ
     # ---- 2D: periodic cubic x Hermite cubic, 512 x 512, 64 fields ------------------------------
     w = W.config3()
     bx, by = D.UniformBSplines(3, True, 0.0, 1.0, 512), D.UniformBSplines(3, False, 0.0, 1.0, 512)
@@ -386,9 +401,38 @@ def measure_configs(peak, reps):
     out["tensor2d_512x512x64"] = {"build_ms": tb, "eval_ms": te, "Gpts_per_s": n2 / (tb + te) / 1e6,
                                   "build_GBps": b_bytes / tb / 1e6, "eval_GBps": e_bytes / te / 1e6,
                                   "hbm_frac": (b_bytes + e_bytes) / (tb + te) / 1e6 / peak}
-    del v, d0, d1, x, c2, y2, ws2
-    # ---- uneven batch: 4096 problems ----------------------------------------------------------
+    # FP32 + refinement (the named precision of this configuration), error against the FP64 build
+    Bxr = D.SplineBuilder(bx, None, 0, 0, precision="fp32_refine", refine_rounds=1)
+    Byr = D.SplineBuilder(by, None, 1, 1, precision="fp32_refine", refine_rounds=1)
+    b2r = D.SplineBuilder2D(Bxr, Byr)
+    c2r = torch.empty_like(c2)
+    tbr = _time_ms(lambda i: b2r(c2r, v, derivs_min2=d0, derivs_max2=d1, workspace=ws2), reps)
+    out["tensor2d_512x512x64"]["fp32_refine_1_round"] = {
+        "build_ms": tbr, "speedup_vs_fp64": tb / tbr, "max_rel_err_vs_fp64": float((c2r - c2).abs().max() / c2.abs().max()),
+        "converged": _converged(Bxr) and _converged(Byr)}
+    # the x-advection of the step (velocity per y row, feet computed in the fused kernel)
+    vy = cu(w["v"])
+    ya = torch.empty_like(v)
+    ex = D.SplineEvaluator(bx)
+    fused_adv = Bx.advect(ex, ya, v, w["dt"], vy, velocity_div=64)
+    ta = _time_ms(lambda i: Bx.advect(ex, ya, v, w["dt"], vy, velocity_div=64), reps)
+    ab = 2 * v.numel() * 8
+    out["advection_x_512x512x64"] = {"ms": ta, "GBps": ab / ta / 1e6, "hbm_frac": ab / ta / 1e6 / peak,
+                                     "schedule": "fused kernel, feet computed in it" if fused_adv else "three kernels"}
+    del v, d0, d1, x, c2, y2, ws2, c2r, ya
+    # ---- uneven batch: 4096 problems, FP32 + refinement (its named precision) -------------------
     probs = W.config4()
+    wr = W.config4_batch(D, probs, precision="fp32_refine", refine_rounds=2)
+    batch = D.UnevenBatch(wr["builders"], wr["evaluators"], wr["nevals"])
+    rinfo = batch.info
+    rv, rlo, rhi, rx = cu(wr["vals"]), cu(wr["dlo"]), cu(wr["dhi"]), cu(wr["coords"])
+    rc = torch.empty((rinfo.total_coefs,), dtype=torch.float64, device=dev)
+    ry = torch.empty((rinfo.total_evals,), dtype=torch.float64, device=dev)
+    rtinf = batch.tune(rv, rlo, rhi, rc, rx, ry, reps=3)
+    trefine = _time_ms(lambda i: batch(rv, rlo, rhi, rc, rx, ry), 10 * reps)
+    r_conv = all(_converged(b) for b in wr["builders"])
+    del batch, rv, rlo, rhi, rx
+    # ---- uneven batch: 4096 problems, FP64 ----------------------------------------------------
     wb = W.config4_batch(D, probs)
     batch = D.UnevenBatch(wb["builders"], wb["evaluators"], wb["nevals"])
     info = batch.info
@@ -411,12 +455,17 @@ def measure_configs(peak, reps):
             ee(yy, xx, cc)
 
     tloop = _time_ms(loop, 2)
+    r_err = float((rc - bc).abs().max() / bc.abs().max())
     ub = 8 * (info.total_vals + info.total_derivs_lo + info.total_derivs_hi + info.total_coefs + 2 * info.total_evals)
     out["uneven_batch_4096"] = {"problems": int(info.count), "points": int(info.total_vals), "evals": int(info.total_evals),
                                 "ms": tbatch, "Gpts_per_s": (info.total_vals + info.total_evals) / 2 / tbatch / 1e6,
                                 "GBps": ub / tbatch / 1e6, "loop_per_problem_fp64_ms": tloop, "speedup_vs_loop": tloop / tbatch,
-                                "schedule": {"threads": tinf.threads, "blocks_per_sm": tinf.blocks_per_sm,
-                                             "order": "largest-first" if tinf.order == 0 else "natural"}}
+                                "schedule": {"warp_schedule": bool(tinf.warp_schedule), "threads": tinf.threads,
+                                             "budget_256_threads_per_sm": tinf.blocks_per_sm,
+                                             "order": "largest-first" if tinf.order == 0 else "natural"},
+                                "fp32_refine_2_rounds": {"ms": trefine, "Gpts_per_s": (info.total_vals + info.total_evals) / 2 / trefine / 1e6,
+                                                        "max_rel_err_vs_fp64_coefs": r_err, "converged": r_conv,
+                                                        "warp_schedule": bool(rtinf.warp_schedule)}}
     del batch, wb, views, bv, blo, bhi, bx_, bc, by_
     # ---- differentiation: periodic cubic 1024 cells, 65536 lines, 1024 points/line ------------
     B, m = 1 << 16, 1024
@@ -436,6 +485,50 @@ def measure_configs(peak, reps):
     bwd_bytes = B * (m + m + 1027 + m + 1024) * 8
     out["adjoint_periodic_cubic_1024x65536"] = {"fwd_ms": tf, "bwd_ms": tb_, "fwd_GBps": fwd_bytes / tf / 1e6,
                                                 "bwd_GBps": bwd_bytes / tb_ / 1e6, "bwd_hbm_frac": bwd_bytes / tb_ / 1e6 / peak}
+    # the forward in FP32 + refinement (this configuration's named precision)
+    br5 = D.SplineBuilder(bs, precision="fp32_refine", refine_rounds=1)
+    c5, y5 = torch.empty_like(c), torch.empty_like(y)
+    tf5 = _time_ms(lambda i: br5.build_and_evaluate(e, c5, v, x, y5), reps)
+    b.build_and_evaluate(e, c, v, x, y)
+    out["adjoint_periodic_cubic_1024x65536"]["fwd_fp32_refine_1_round"] = {
+        "ms": tf5, "speedup_vs_fp64": tf / tf5, "max_rel_err_vs_fp64_values": float((y5 - y).abs().max() / y.abs().max()),
+        "converged": _converged(br5)}
+    del x, g, v, c, y, gv, gx, c5, y5
+    # ---- the advection step of periodic cubic 1000 cells x 1000 lines (feet in the kernel) ----
+    bs1 = D.UniformBSplines(3, True, 0.0, 1.0, 1000)
+    b1, e1 = D.SplineBuilder(bs1), D.SplineEvaluator(bs1)
+    sets = 8
+    f_in = [torch.randn((1000, 1000), dtype=torch.float64, device=dev) for _ in range(sets)]
+    f_out = [torch.empty((1000, 1000), dtype=torch.float64, device=dev) for _ in range(sets)]
+    fused1 = b1.advect(e1, f_out[0], f_in[0], 0.37e-3, 1.0)
+    ta1 = _time_ms(lambda i: b1.advect(e1, f_out[i], f_in[i], 0.37e-3, 1.0), 10 * reps, sets)
+    ab1 = 2 * 1000 * 1000 * 8
+    out["advection_periodic_cubic_1000x1000"] = {"ms": ta1, "GBps": ab1 / ta1 / 1e6, "hbm_frac": ab1 / ta1 / 1e6 / peak,
+                                                 "schedule": "fused kernel, feet computed in it" if fused1 else "three kernels",
+                                                 "note": "8 rotating buffer sets (128 MB)"}
+    del f_in, f_out
+    # ---- 3D: periodic cubic x Hermite cubic x Greville cubic, 96^3 cells, 16 fields ----------
+    n3, F = 96, 16
+    b3 = [D.UniformBSplines(3, True, 0.0, 1.0, n3), D.UniformBSplines(3, False, 0.0, 1.0, n3),
+          D.UniformBSplines(3, False, 0.0, 1.0, n3)]
+    B3 = [D.SplineBuilder(b3[0]), D.SplineBuilder(b3[1], None, 1, 1), D.SplineBuilder(b3[2], None, 3, 3)]
+    bld3 = D.SplineBuilder3D(*B3)
+    np3 = [bb.npoints for bb in B3]
+    v3 = torch.randn((np3[0], np3[1], np3[2], F), dtype=torch.float64, device=dev)
+    dm = torch.randn((np3[0], 1, np3[2], F), dtype=torch.float64, device=dev)
+    dM = torch.randn((np3[0], 1, np3[2], F), dtype=torch.float64, device=dev)
+    c3 = torch.empty((b3[0].size, b3[1].size, b3[2].size, F), dtype=torch.float64, device=dev)
+    ws3 = torch.empty(bld3.workspace_bytes(F) // 8 + 1, dtype=torch.float64, device=dev)
+    tb3 = _time_ms(lambda i: bld3(c3, v3, workspace=ws3, derivs_min2=dm, derivs_max2=dM), reps)
+    ev3 = D.SplineEvaluator3D(*[D.SplineEvaluator(bb) for bb in b3])
+    x3 = torch.rand((np3[0] * np3[1] * np3[2] // 4, F, 3), dtype=torch.float64, device=dev)
+    y3 = torch.empty((x3.shape[0], F), dtype=torch.float64, device=dev)
+    te3 = _time_ms(lambda i: ev3(y3, x3, c3), reps)
+    bb3 = (v3.numel() + dm.numel() + dM.numel() + c3.numel()) * 8
+    eb3 = (c3.numel() + x3.numel() + y3.numel()) * 8
+    out["tensor3d_96cubed_x16"] = {"build_ms": tb3, "eval_ms": te3, "build_GBps": bb3 / tb3 / 1e6,
+                                   "eval_points": int(y3.numel()), "eval_Gpts_per_s": y3.numel() / te3 / 1e6,
+                                   "eval_GBps_algorithmic": eb3 / te3 / 1e6}
     return out
 
 

@@ -63,7 +63,7 @@ class UnevenInfo(C.Structure):
     _fields_ = [("count", C.c_int64), ("total_vals", C.c_int64), ("total_derivs_lo", C.c_int64),
                 ("total_derivs_hi", C.c_int64), ("total_coefs", C.c_int64), ("total_evals", C.c_int64),
                 ("threads", C.c_int32), ("blocks_per_sm", C.c_int32), ("order", C.c_int32),
-                ("shared_bytes", C.c_int32), ("tuned_us", C.c_double)]
+                ("shared_bytes", C.c_int32), ("tuned_us", C.c_double), ("warp_schedule", C.c_int32)]
 
 
 _vp = C.c_void_p

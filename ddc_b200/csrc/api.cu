@@ -765,7 +765,7 @@ ddcb_status ddcb_batch_uneven_get_info(ddcb_uneven_batch h, ddcb_uneven_info* in
     return guarded(__func__, [&] {
         require(h != nullptr && info != nullptr, "NULL argument");
         int64_t tot[6];
-        int sch[4];
+        int sch[5];
         double us = 0.0;
         ddcb::uneven_info(*h->b, tot, sch, &us);
         info->count = tot[0];
@@ -779,6 +779,7 @@ ddcb_status ddcb_batch_uneven_get_info(ddcb_uneven_batch h, ddcb_uneven_info* in
         info->order = sch[2];
         info->shared_bytes = sch[3];
         info->tuned_us = us;
+        info->warp_schedule = sch[4];
     });
 }
 
@@ -796,7 +797,7 @@ static void check_uneven_buffers(ddcb_uneven_batch h, const double* vals, const 
 {
     require(h != nullptr, "batch is NULL");
     int64_t tot[6];
-    int sch[4];
+    int sch[5];
     double us;
     ddcb::uneven_info(*h->b, tot, sch, &us);
     require(tot[1] == 0 || vals, "vals is NULL");

@@ -176,7 +176,7 @@ struct Builder
                                    // lower derivatives (nbv_lo), upper derivatives (nbv_hi)]
     double* d_points = nullptr;    // the interpolation points on the device (inside d_block)
     unsigned* d_status = nullptr;  // device status word (inside d_block): bit 0 = not converged
-    double cond_est = 0.0;         // estimate of ||A^-1||_inf
+    double cond_est = 0.0;         // estimate of cond_inf(A) = ||A||_inf ||A^-1||_inf
     RhsMap rhs {};
     std::string structure;
     void* host_private = nullptr;  // host factorisation (plan.cpp)
@@ -301,7 +301,7 @@ void tune_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, do
 size_t build2d_workspace_bytes(Builder const& b1, Builder const& b2, int64_t nbatch);
 void launch_build2d(Builder const& b1, Builder const& b2, double* coefs, double const* vals, double const* dmin1,
                     double const* dmax1, double const* dmin2, double const* dmax2, double const* m11, double const* m21,
-                    double const* m12, double const* m22, int64_t B, double* ws, cudaStream_t s);
+                    double const* m12, double const* m22, int64_t B, double* ws, cudaStream_t s, int64_t max_group = 0);
 void launch_eval2d(Evaluator const& e1, Evaluator const& e2, int o1, int o2, double* out, double const* coords,
                    double const* coefs, int64_t m, int64_t B, cudaStream_t s);
 void launch_integrate2d(Evaluator const& e1, Evaluator const& e2, double* out, double const* coefs, int64_t B, cudaStream_t s);

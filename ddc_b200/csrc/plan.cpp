@@ -927,6 +927,51 @@ struct BuilderPrivate
     SparseRows ref_rows; // the assembled system in the reference's row / column order
 };
 
+// The system the reference solves on uniform bases. SplineBuilder::allocate_matrix passes
+// pds = is_uniform() to the matrix maker (spline_builder.hpp:740-764), whose centre block -- rows
+// and columns [top, n - bottom) of the 3x3 layout, or [0, n - max(kl, ku)) of the periodic 2x2
+// layout, kl = ku = degree / 2 -- is then a symmetric band (splines_linear_problem_pds_band.cpp,
+// pds_tridiag.cpp: entries (i, j) and (j, i) share one slot, entries beyond the band are dropped).
+// build_matrix_system writes the rows in order (spline_builder.hpp:784-886), so each slot keeps
+// its lower-triangle value when both were written. On the interpolation matrix of a uniform basis
+// the two differ by round-off only, but that round-off moves the solution by up to cond(A) times
+// it; solving the reference's symmetric block keeps the result within cond(A) eps of it.
+static void symmetrize_like_reference(SparseRows& rows, Builder const& bl, long top, long bottom)
+{
+    BasisDesc const& D = bl.basis.desc;
+    if (!D.uniform) return;
+    long const n = bl.n, kd = D.degree / 2;
+    long q0, q1;
+    if (D.periodic) {
+        long const bot = kd, tp = n - bot; // make_new_periodic_band_matrix: bottom = max(kl, ku)
+        // its dense fallback keeps every entry as written
+        if (bot * (n + tp) + (2 * kd + kd + 1) * tp >= n * n) return;
+        q0 = 0;
+        q1 = n - bot;
+    } else {
+        q0 = top;
+        q1 = n - bottom;
+    }
+    for (long i = q0; i < q1; ++i)
+        for (long j = i + 1; j < std::min(q1, i + kd + 1); ++j) {
+            auto lo = rows[j].find(i);
+            auto up = rows[i].find(j);
+            // the later row (j) overwrites the slot when it wrote it
+            double const v = lo != rows[j].end() ? lo->second : (up != rows[i].end() ? up->second : 0.0);
+            if (v != 0.0) {
+                rows[i][j] = v;
+                rows[j][i] = v;
+            }
+        }
+    // beyond the band, the centre block keeps nothing
+    for (long i = q0; i < q1; ++i)
+        for (auto it = rows[i].begin(); it != rows[i].end();) {
+            long const j = it->first;
+            if (j >= q0 && j < q1 && std::labs(j - i) > kd) it = rows[i].erase(it);
+            else ++it;
+        }
+}
+
 // An estimate of ||A^-1||_inf = ||A^-T||_1 by Higham's 1-norm estimator (N. J. Higham, ACM TOMS 14
 // (1988) 381-396, after Hager 1984): a few solves with A^T and A on sign vectors. It bounds the
 // forward error of a refined solution from its residual: |x - x*| <= ||A^-1|| |b - A x|.
@@ -1024,6 +1069,7 @@ Builder* create_builder_host(Basis const& basis, double const* pts, long npts, i
             bottom = block(hi, b->nbe_hi);
             if (top + bottom >= b->n) top = bottom = 0;
         }
+        symmetrize_like_reference(rows, *b, top, bottom);
         b->rrot = int(top);
         b->crot = int(top);
         if (top) {
@@ -1036,6 +1082,7 @@ Builder* create_builder_host(Basis const& basis, double const* pts, long npts, i
         auto* priv = new BuilderPrivate();
         b->host_private = priv;
         priv->ref_rows = assemble(*b);
+        symmetrize_like_reference(priv->ref_rows, *b, top, bottom);
         priv->fwd.analyse(rows, D.periodic != 0, top + bottom);
         priv->fwd.make_tables(b->nchunk_req);
         priv->adj.analyse(transpose_rows(rows), D.periodic != 0, top + bottom);

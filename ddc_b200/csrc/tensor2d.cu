@@ -20,11 +20,20 @@ namespace ddcb {
 
 namespace {
 
-int64_t group_fields(Builder const& b1, Builder const& b2, int64_t nbatch)
+// Fields per group: the x1-pass result of a group stays near 40 MiB (L2-sized), and at most
+// max_group fields (0: no cap).
+int64_t group_fields(Builder const& b1, Builder const& b2, int64_t nbatch, int64_t max_group = 0)
 {
     int64_t const per_field = b1.basis.size() * int64_t(b2.points.size() + b2.nbv_lo + b2.nbv_hi) * 8;
     int64_t g = std::max<int64_t>(1, (int64_t(40) << 20) / std::max<int64_t>(per_field, 1));
+    if (max_group > 0) g = std::min(g, max_group);
     return std::min(g, nbatch);
+}
+
+// Workspace bytes for groups of G fields.
+size_t workspace_for_group(Builder const& b1, Builder const& b2, int64_t nbatch, int64_t G)
+{
+    return size_t(b1.basis.size()) * (size_t(b2.points.size()) * size_t(G) + size_t(b2.nbv_lo + b2.nbv_hi) * size_t(nbatch)) * 8;
 }
 
 } // namespace
@@ -33,19 +42,18 @@ int64_t group_fields(Builder const& b1, Builder const& b2, int64_t nbatch)
 // results of the dim-2 derivative slabs of every field, (s1, nlo2, B) and (s1, nhi2, B).
 size_t build2d_workspace_bytes(Builder const& b1, Builder const& b2, int64_t nbatch)
 {
-    int64_t const G = group_fields(b1, b2, nbatch);
-    return size_t(b1.basis.size()) * (size_t(b2.points.size()) * size_t(G) + size_t(b2.nbv_lo + b2.nbv_hi) * size_t(nbatch)) * 8;
+    return workspace_for_group(b1, b2, nbatch, group_fields(b1, b2, nbatch));
 }
 
 void launch_build2d(Builder const& b1, Builder const& b2, double* coefs, double const* vals, double const* dmin1,
                     double const* dmax1, double const* dmin2, double const* dmax2, double const* m11, double const* m21,
-                    double const* m12, double const* m22, int64_t B, double* ws, cudaStream_t s)
+                    double const* m12, double const* m22, int64_t B, double* ws, cudaStream_t s, int64_t max_group)
 {
     int64_t const np1 = int64_t(b1.points.size()), np2 = int64_t(b2.points.size());
     int64_t const s1 = b1.basis.size(), s2 = b2.basis.size();
     int64_t const nlo1 = b1.nbv_lo, nhi1 = b1.nbv_hi, nlo2 = b2.nbv_lo, nhi2 = b2.nbv_hi;
     bool const her_lo2 = b2.lo == DDCB_HERMITE && nlo2 > 0, her_hi2 = b2.hi == DDCB_HERMITE && nhi2 > 0;
-    int64_t const G0 = group_fields(b1, b2, B);
+    int64_t const G0 = group_fields(b1, b2, B, max_group);
     Lines const none {0, 1, 0, 0, 0};
     double* S1 = ws;                        // (s1, np2, G0): one group's x1 pass over the values
     double* S1lo = S1 + s1 * np2 * G0;      // (s1, nlo2, B): every field's lower derivative slab
@@ -269,14 +277,22 @@ void* g_scratch_addr[256] = {};
 
 // Device address of the scratch array on the current device, looked up once per device. The host
 // symbol g_build2d_scratch is only a stand-in for the device array; kernels must be given the
-// address the runtime reports for the current device.
-double* static_scratch_for_current_device()
+// address the runtime reports for the current device. The lookup may load the library's device
+// code, which must not happen while `s` is being captured into a graph: a first call made under
+// capture is refused with a message instead.
+double* static_scratch_for_current_device(cudaStream_t s)
 {
     int dev = 0;
     DDCB_CUDA_CHECK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 256) throw Error(DDCB_ERR_UNSUPPORTED, "device ordinal out of range");
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
     if (g_scratch_addr[dev] == nullptr) {
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        DDCB_CUDA_CHECK(cudaStreamIsCapturing(s, &cap));
+        if (cap != cudaStreamCaptureStatusNone)
+            throw Error(DDCB_ERR_INVALID_ARGUMENT, "the first ddcb_build2d_static_scratch call on a device looks up the "
+                                                   "static scratch and must run outside stream capture: make one call "
+                                                   "before capturing");
         void* p = nullptr;
         cudaError_t const e = cudaGetSymbolAddress(&p, g_build2d_scratch);
         if (e != cudaSuccess || p == nullptr)
@@ -294,13 +310,17 @@ void launch_build2d_static(Builder const& b1, Builder const& b2, double* coefs, 
                            double const* dmax1, double const* dmin2, double const* dmax2, double const* m11,
                            double const* m21, double const* m12, double const* m22, int64_t B, cudaStream_t s)
 {
-    size_t const need = build2d_workspace_bytes(b1, b2, B);
+    // the largest group of fields whose scratch fits the array; refused only when one field does not
+    int64_t G = group_fields(b1, b2, B);
+    while (G > 1 && workspace_for_group(b1, b2, B, G) > kStaticScratchBytes) G = std::max<int64_t>(1, G / 2);
+    while (G > 1 && workspace_for_group(b1, b2, B, G) > kStaticScratchBytes) --G;
+    size_t const need = workspace_for_group(b1, b2, B, G);
     if (need > kStaticScratchBytes)
-        throw Error(DDCB_ERR_UNSUPPORTED, "this 2D build needs " + std::to_string(need) + " bytes of scratch, more than the "
-                                              + std::to_string(kStaticScratchBytes)
+        throw Error(DDCB_ERR_UNSUPPORTED, "this 2D build needs " + std::to_string(need) + " bytes of scratch with one field per "
+                                              "group, more than the " + std::to_string(kStaticScratchBytes)
                                               + " bytes of the library's static scratch; use ddcb_build2d with a workspace");
-    double* ws = static_scratch_for_current_device();
-    launch_build2d(b1, b2, coefs, vals, dmin1, dmax1, dmin2, dmax2, m11, m21, m12, m22, B, ws, s);
+    double* ws = static_scratch_for_current_device(s);
+    launch_build2d(b1, b2, coefs, vals, dmin1, dmax1, dmin2, dmax2, m11, m21, m12, m22, B, ws, s, G);
 }
 
 } // namespace ddcb

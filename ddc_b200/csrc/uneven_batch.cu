@@ -3,25 +3,31 @@
 //
 // Each problem is one line: a builder (its device factor tables) and an evaluator, with its
 // samples, derivatives, coefficients, coordinates and values packed one after another in flat
-// arrays. Problems are grouped by the band shape of their factors (the solve is compiled per
-// shape: one kernel holding every shape's solve spills registers). Each group gets a persistent
-// kernel with a fixed grid (its share of blocks_per_sm x SMs, in proportion to its work); every
-// block takes the group's next problem from a counter (largest-first order by default, so the long
-// problems start early and the short ones fill the tail), builds it in shared memory with the same
-// chunked tile solve as the batched builder (a line pair whose second line is empty), stores its
-// coefficients and evaluates its points from the solved tile. The per-problem description is
-// copied into shared memory once per problem, so the solve reads its tables' addresses from there.
+// arrays. Problems are grouped by the band shape of their factors and their arithmetic (the solve
+// is compiled per shape: one kernel holding every shape's solve spills registers; FP64 or FP32 with
+// FP64 refinement), and by block size: under the warp schedule a problem's block has one thread
+// per chunk of its plan, rounded up to a warp, so short problems (<= 32 chunks) run one warp each,
+// many per SM, with barriers that cost a warp's; under the block schedule every block has
+// `threads` threads. Each group gets a persistent kernel with a fixed grid (its share, by work, of a
+// per-SM thread budget); every block takes the group's next problem from a counter (largest-first
+// order by default, so the long problems start early and the short ones fill the tail), builds it
+// in shared memory with the chunked tile solve of the batched builder (the chunks' carries chained
+// by the log-depth scan across the block's threads), stores its coefficients and evaluates its
+// points from the solved tile. The per-problem description is copied into shared memory once per
+// problem, so the solve reads its tables' addresses from there.
 //
 // ddcb_batch_uneven_run launches a CUDA graph holding the counter reset and the group kernels,
 // which run concurrently; the graph is rebuilt only when the buffers, stream or schedule change.
-// ddcb_batch_uneven_tune times the candidate schedules (block size, blocks per SM, queue order),
-// each as the graph it would run as, on the caller's buffers and keeps the fastest.
+// ddcb_batch_uneven_tune times the candidate schedules (warp or block schedule, block size, the
+// per-SM thread budget, queue order), each as the graph it would run as, on the caller's buffers
+// and keeps the fastest.
 #include <algorithm>
 #include <cmath>
 #include <numeric>
 
 #include "build_device.cuh"
 #include "eval_device.cuh"
+#include "refine_device.cuh"
 
 namespace ddcb {
 
@@ -35,6 +41,7 @@ struct UnevenProblem
     EvalBasis eb;
     int ex_lo, ex_hi;
     int shape;             // index into kShapes
+    int rounds;            // refinement rounds (FP32 solve); -1: FP64 solve
     int degree, uniform;
     int m;                 // evaluation points
     int64_t x_off, out_off;
@@ -80,7 +87,7 @@ __device__ __forceinline__ void eval_any(int degree, int uniform, EvalBasis cons
     }
 }
 
-template <int KL, int KU>
+template <int KL, int KU, bool REFINE>
 __global__ void __launch_bounds__(512) uneven_kernel(const __grid_constant__ UnevenArgs A)
 {
     extern __shared__ __align__(16) double smem[];
@@ -106,8 +113,12 @@ __global__ void __launch_bounds__(512) uneven_kernel(const __grid_constant__ Une
             sp.args.nct = blockDim.x / 2;
         }
         __syncthreads();
-        gather_tile<2>(sp.args, smem);
-        solve_in_tile<2, KL, KU>(sp.args.t, 0, smem);
+        if constexpr (REFINE) {
+            refine_tile<2, KL, KU>(sp.args, smem, sp.rounds);
+        } else {
+            gather_tile<2>(sp.args, smem);
+            solve_in_tile<2, KL, KU>(sp.args.t, 0, smem);
+        }
         store_tile<2>(sp.args, smem);
         CoefRotated const acc {smem, 2, sp.args.t.n, sp.args.r.srot};
         eval_any(sp.degree, sp.uniform, sp.eb, sp.ex_lo, sp.ex_hi, acc, A.coords + sp.x_off, A.out + sp.out_off, sp.m);
@@ -117,27 +128,34 @@ __global__ void __launch_bounds__(512) uneven_kernel(const __grid_constant__ Une
 
 using UnevenKernel = void (*)(UnevenArgs);
 
-UnevenKernel kernel_of(int shape)
+template <bool R>
+UnevenKernel kernel_of_r(int shape)
 {
     switch (shape) {
-    case 0: return uneven_kernel<1, 1>;
-    case 1: return uneven_kernel<1, 2>;
-    case 2: return uneven_kernel<2, 2>;
-    case 3: return uneven_kernel<3, 3>;
-    case 4: return uneven_kernel<1, 4>;
-    case 5: return uneven_kernel<2, 4>;
-    case 6: return uneven_kernel<4, 4>;
-    case 7: return uneven_kernel<3, 6>;
-    case 8: return uneven_kernel<1, 8>;
-    case 9: return uneven_kernel<2, 8>;
-    default: return uneven_kernel<4, 8>;
+    case 0: return uneven_kernel<1, 1, R>;
+    case 1: return uneven_kernel<1, 2, R>;
+    case 2: return uneven_kernel<2, 2, R>;
+    case 3: return uneven_kernel<3, 3, R>;
+    case 4: return uneven_kernel<1, 4, R>;
+    case 5: return uneven_kernel<2, 4, R>;
+    case 6: return uneven_kernel<4, 4, R>;
+    case 7: return uneven_kernel<3, 6, R>;
+    case 8: return uneven_kernel<1, 8, R>;
+    case 9: return uneven_kernel<2, 8, R>;
+    default: return uneven_kernel<4, 8, R>;
     }
 }
 
+UnevenKernel kernel_of(int shape, bool refine) { return refine ? kernel_of_r<true>(shape) : kernel_of_r<false>(shape); }
+
 size_t problem_smem(UnevenProblem const& p)
 {
-    return sizeof(double) * tile_doubles(p.args.t, 2, kShapes[p.shape][0], kShapes[p.shape][1]);
+    int const kl = kShapes[p.shape][0], ku = kShapes[p.shape][1];
+    return p.rounds >= 0 ? refine_smem(p.args.t, 2, kl, ku) : sizeof(double) * tile_doubles(p.args.t, 2, kl, ku);
 }
+
+// The block of a problem under the warp schedule: one thread per chunk, whole warps.
+int warp_class(int nchunk) { return std::max(32, (nchunk + 31) / 32 * 32); }
 
 } // namespace
 
@@ -147,9 +165,10 @@ struct UnevenBatch
     int64_t count = 0;
     std::vector<int64_t> vals_off, dlo_off, dhi_off, coef_off, x_off; // count + 1 prefix sums
     UnevenProblem* d_probs = nullptr;
-    // per band-shape group: its problems in two queue orders (largest-first, then natural) at
-    // d_order + 2*gfirst[g] and d_order + 2*gfirst[g] + gsize[g]; its counter d_counter[g]
-    std::vector<int> gshape, gfirst, gsize;
+    // per group (band shape, arithmetic, warp-schedule block size): its problems in two queue
+    // orders (largest-first, then natural) at d_order + 2*gfirst[g] and d_order + 2*gfirst[g] +
+    // gsize[g]; its counter d_counter[g]
+    std::vector<int> gshape, grefine, gclass, gfirst, gsize;
     std::vector<double> gcost;
     std::vector<size_t> gsmem;
     int* d_order = nullptr;
@@ -157,8 +176,9 @@ struct UnevenBatch
     size_t smem = 0;
     int max_chunks = 0;
     // schedule
+    int warp = 1;              // 1: blocks sized to each problem's chunks; 0: `threads` for every block
     int threads = 256;
-    int blocks_per_sm = 0;     // 0: as many as fit
+    int blocks_per_sm = 0;     // per-SM budget in units of 256 threads (0: as many blocks as fit)
     int order = 0;             // 0 largest-first, 1 natural
     double tuned_us = 0.0;
     // cached graph
@@ -166,7 +186,7 @@ struct UnevenBatch
     cudaGraphExec_t exec = nullptr;
     UnevenArgs key {};
     cudaStream_t key_stream = nullptr;
-    int key_threads = 0, key_blocks = 0, key_order = -1;
+    int key_threads = 0, key_blocks = 0, key_order = -1, key_warp = -1;
 };
 
 namespace {
@@ -179,17 +199,24 @@ int sm_count()
     return sms;
 }
 
-// Blocks of group g's kernel: its share (by work) of per_sm (0: as many as fit) blocks per SM
-// over the SMs, at least one, at most its problem count.
+// Block size of group g under the current schedule.
+int group_threads(UnevenBatch const& b, int g)
+{
+    int const c = b.gclass[size_t(g)];
+    return b.warp ? c : std::max(b.threads, c);
+}
+
+// Blocks of group g's kernel: its share (by work) of the per-SM budget (blocks_per_sm x 256
+// threads; 0: as many blocks as fit) over the SMs, at least one, at most its problem count.
 int group_blocks(UnevenBatch const& b, int g, int threads, int per_sm)
 {
-    UnevenKernel k = kernel_of(b.gshape[size_t(g)]);
+    UnevenKernel k = kernel_of(b.gshape[size_t(g)], b.grefine[size_t(g)] != 0);
     size_t const sm = b.gsmem[size_t(g)];
     if (sm > 48 * 1024) DDCB_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
     int fit = 0;
     DDCB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k, threads, sm));
     if (fit < 1) throw Error(DDCB_ERR_UNSUPPORTED, "the largest problem's tile does not fit in shared memory");
-    int const per = per_sm > 0 ? std::min(per_sm, fit) : fit;
+    int const per = per_sm > 0 ? std::min(std::max(1, per_sm * 256 / threads), fit) : fit;
     double total = 0.0;
     for (double c : b.gcost) total += c;
     double const share = total > 0.0 ? b.gcost[size_t(g)] / total : 1.0;
@@ -240,12 +267,12 @@ UnevenBatch* create_uneven_batch(Builder const* const* builders, Evaluator const
             Evaluator const& ev = *evals[i];
             std::string const who = "problem " + std::to_string(i) + ": ";
             if (bl.device != b->device || ev.device != b->device) throw Error(DDCB_ERR_INVALID_ARGUMENT, who + "created for another device");
-            if (bl.precision != DDCB_FP64) throw Error(DDCB_ERR_UNSUPPORTED, who + "the uneven batch runs the FP64 solve");
             if (ev.basis.desc.degree != bl.basis.desc.degree || ev.basis.desc.ncells != bl.basis.desc.ncells
                 || ev.basis.desc.periodic != bl.basis.desc.periodic || ev.basis.desc.uniform != bl.basis.desc.uniform)
                 throw Error(DDCB_ERR_INVALID_ARGUMENT, who + "builder and evaluator use different bases");
             if (nevals[i] < 0 || nevals[i] > (int64_t(1) << 30)) throw Error(DDCB_ERR_INVALID_ARGUMENT, who + "bad evaluation count");
             UnevenProblem& p = probs[size_t(i)];
+            p.rounds = bl.precision == DDCB_FP32_REFINE ? bl.refine_rounds : -1;
             p.shape = -1;
             for (int sh = 0; sh < kNumShapes; ++sh)
                 if (kShapes[sh][0] == bl.tables.kl && kShapes[sh][1] == bl.tables.ku) p.shape = sh;
@@ -287,32 +314,37 @@ UnevenBatch* create_uneven_batch(Builder const* const* builders, Evaluator const
             cost[size_t(i)] = 64.0 + double(np) * (kShapes[p.shape][0] + kShapes[p.shape][1] + 2) / 8.0
                               + double(nevals[i]) * (p.degree + 1) / 8.0;
         }
-        // groups by band shape (splitting them further by tile size, so that short problems ask
-        // for less shared memory, measured slower: the groups' grids then balance worse); queue
-        // orders within each group
+        // groups by band shape, arithmetic and warp-schedule block size (the tile of a group is
+        // sized to its largest problem); queue orders within each group
         std::vector<int> order;
         for (int sh = 0; sh < kNumShapes; ++sh) {
-            std::vector<int> members;
-            size_t smem = 0;
-            double c = 0.0;
-            for (int64_t i = 0; i < count; ++i) {
-                UnevenProblem const& p = probs[size_t(i)];
-                if (p.shape != sh) continue;
-                members.push_back(int(i));
-                smem = std::max(smem, problem_smem(p));
-                c += cost[size_t(i)];
+            for (int rf = 0; rf < 2; ++rf) {
+                for (int cls = 32; cls <= 512; cls += 32) {
+                    std::vector<int> members;
+                    size_t smem = 0;
+                    double c = 0.0;
+                    for (int64_t i = 0; i < count; ++i) {
+                        UnevenProblem const& p = probs[size_t(i)];
+                        if (p.shape != sh || (p.rounds >= 0) != (rf == 1) || warp_class(p.args.t.nchunk) != cls) continue;
+                        members.push_back(int(i));
+                        smem = std::max(smem, problem_smem(p));
+                        c += cost[size_t(i)];
+                    }
+                    if (members.empty()) continue;
+                    b->gshape.push_back(sh);
+                    b->grefine.push_back(rf);
+                    b->gclass.push_back(cls);
+                    b->gfirst.push_back(int(order.size() / 2));
+                    b->gsize.push_back(int(members.size()));
+                    b->gcost.push_back(c);
+                    b->gsmem.push_back((smem + 15) & ~size_t(15));
+                    b->smem = std::max(b->smem, b->gsmem.back());
+                    std::vector<int> lpt = members;
+                    std::stable_sort(lpt.begin(), lpt.end(), [&](int x, int y) { return cost[size_t(x)] > cost[size_t(y)]; });
+                    order.insert(order.end(), lpt.begin(), lpt.end());
+                    order.insert(order.end(), members.begin(), members.end());
+                }
             }
-            if (members.empty()) continue;
-            b->gshape.push_back(sh);
-            b->gfirst.push_back(int(order.size() / 2));
-            b->gsize.push_back(int(members.size()));
-            b->gcost.push_back(c);
-            b->gsmem.push_back((smem + 15) & ~size_t(15));
-            b->smem = std::max(b->smem, b->gsmem.back());
-            std::vector<int> lpt = members;
-            std::stable_sort(lpt.begin(), lpt.end(), [&](int x, int y) { return cost[size_t(x)] > cost[size_t(y)]; });
-            order.insert(order.end(), lpt.begin(), lpt.end());
-            order.insert(order.end(), members.begin(), members.end());
         }
         if (count > 0) {
             DDCB_CUDA_CHECK(cudaMalloc(&b->d_probs, sizeof(UnevenProblem) * size_t(count)));
@@ -363,6 +395,7 @@ void uneven_info(UnevenBatch const& b, int64_t* totals, int* schedule, double* t
     schedule[1] = b.blocks_per_sm;
     schedule[2] = b.order;
     schedule[3] = int(b.smem);
+    schedule[4] = b.warp;
     *tuned_us = b.tuned_us;
 }
 
@@ -374,7 +407,7 @@ void run_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, dou
     bool const stale = !b.exec || key.vals != b.key.vals || key.dlo != b.key.dlo || key.dhi != b.key.dhi
                        || key.coefs != b.key.coefs || key.coords != b.key.coords || key.out != b.key.out
                        || s != b.key_stream || b.threads != b.key_threads || b.blocks_per_sm != b.key_blocks
-                       || b.order != b.key_order;
+                       || b.order != b.key_order || b.warp != b.key_warp;
     if (stale) {
         drop_graph(b);
         DDCB_CUDA_CHECK(cudaGraphCreate(&b.graph, 0));
@@ -391,9 +424,10 @@ void run_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, dou
             UnevenArgs args = make_args(b, g, b.order, vals, dlo, dhi, coefs, coords, out);
             void* params[] = {&args};
             cudaKernelNodeParams kp {};
-            kp.func = reinterpret_cast<void*>(kernel_of(b.gshape[size_t(g)]));
-            kp.gridDim = dim3(unsigned(group_blocks(b, g, b.threads, b.blocks_per_sm)));
-            kp.blockDim = dim3(unsigned(b.threads));
+            int const th = group_threads(b, g);
+            kp.func = reinterpret_cast<void*>(kernel_of(b.gshape[size_t(g)], b.grefine[size_t(g)] != 0));
+            kp.gridDim = dim3(unsigned(group_blocks(b, g, th, b.blocks_per_sm)));
+            kp.blockDim = dim3(unsigned(th));
             kp.sharedMemBytes = unsigned(b.gsmem[size_t(g)]);
             kp.kernelParams = params;
             cudaGraphNode_t knode = nullptr;
@@ -405,6 +439,7 @@ void run_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, dou
         b.key_threads = b.threads;
         b.key_blocks = b.blocks_per_sm;
         b.key_order = b.order;
+        b.key_warp = b.warp;
     }
     DDCB_CUDA_CHECK(cudaGraphLaunch(b.exec, s));
 }
@@ -418,16 +453,26 @@ void tune_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, do
     DDCB_CUDA_CHECK(cudaEventCreate(&e0));
     DDCB_CUDA_CHECK(cudaEventCreate(&e1));
     double best = 1e300;
-    int const t0 = b.threads, p0 = b.blocks_per_sm, o0 = b.order;
-    int bt = t0, bb = p0, bo = o0;
+    int const t0 = b.threads, p0 = b.blocks_per_sm, o0 = b.order, w0 = b.warp;
+    int bt = t0, bb = p0, bo = o0, bw = w0;
     try {
-        // each candidate runs as the graph it would be launched as (the group kernels concurrent)
-        for (int threads : {128, 256, 512}) {
-            if (threads < b.max_chunks) continue; // one thread per chunk of the longest problem
-            for (int per : {1, 2, 3, 4, 6, 8}) {
+        // each candidate runs as the graph it would be launched as (the group kernels concurrent):
+        // the warp schedule with per-SM budgets, and the block schedule with block sizes and budgets
+        struct Cand
+        {
+            int warp, threads, per;
+        };
+        std::vector<Cand> cands;
+        for (int per : {2, 4, 6, 8}) cands.push_back({1, 256, per});
+        for (int threads : {128, 256, 512})
+            for (int per : {1, 2, 4, 8}) cands.push_back({0, threads, per});
+        for (Cand const& cd : cands) {
+            if (!cd.warp && cd.threads < b.max_chunks) continue; // one thread per chunk of the longest problem
+            {
                 for (int order : {0, 1}) {
-                    b.threads = threads;
-                    b.blocks_per_sm = per;
+                    b.warp = cd.warp;
+                    b.threads = cd.threads;
+                    b.blocks_per_sm = cd.per;
                     b.order = order;
                     run_uneven_batch(b, vals, dlo, dhi, coefs, coords, out, s); // builds the graph; warm-up
                     DDCB_CUDA_CHECK(cudaEventRecord(e0, s));
@@ -439,9 +484,10 @@ void tune_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, do
                     double const us = 1e3 * ms / reps;
                     if (us < best) {
                         best = us;
-                        bt = threads;
-                        bb = per;
+                        bt = cd.threads;
+                        bb = cd.per;
                         bo = order;
+                        bw = cd.warp;
                     }
                 }
             }
@@ -452,6 +498,7 @@ void tune_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, do
         b.threads = t0;
         b.blocks_per_sm = p0;
         b.order = o0;
+        b.warp = w0;
         throw;
     }
     cudaEventDestroy(e0);
@@ -459,6 +506,7 @@ void tune_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, do
     b.threads = bt;
     b.blocks_per_sm = bb;
     b.order = bo;
+    b.warp = bw;
     if (best < 1e300) b.tuned_us = best;
 }
 

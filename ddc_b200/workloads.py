@@ -105,7 +105,7 @@ def config3(nfields: int = 64, ncells: int = 512):
     feet_y = y[None, :, None] + np.zeros((ncells, 1, nfields))
     coords = np.ascontiguousarray(np.stack([feet_x, feet_y], axis=-1))
     return dict(x=x, y=y, vals=np.ascontiguousarray(vals), dmin2=dmin2, dmax2=dmax2, coords=coords, ncells=ncells,
-                nfields=nfields)
+                nfields=nfields, v=v, dt=dt)
 
 
 def config4(count: int = 4096, nmin: int = 32, nmax: int = 4096, seed: int = 0xDDC0 + 4):
@@ -146,10 +146,11 @@ def config4_samples(p, points, nbv_lo, nbv_hi):
     return vals, lo, hi
 
 
-def config4_batch(D, probs):
+def config4_batch(D, probs, precision="fp64", refine_rounds=2):
     """Builders, evaluators and packed host inputs (flat arrays in problem order) of config4
     problems; `D` is the ddc_b200 package. Each builder solves one line: tile width 2 and about 16
-    rows per chunk."""
+    rows per chunk (so problems under 512 rows have at most 32 chunks: one warp each under the warp
+    schedule). precision "fp32_refine" builds every problem in FP32 with FP64 refinement."""
     closure = {"periodic": 0, "hermite": 1, "greville": 3}
     builders, evaluators, nevals = [], [], []
     vals, dlo, dhi, coords = [], [], [], []
@@ -158,7 +159,8 @@ def config4_batch(D, probs):
         per = p["closure"] == "periodic"
         bs = D.UniformBSplines(d, per, 0.0, 1.0, n) if p["uniform"] else D.NonUniformBSplines(d, per, p["breaks"])
         c = closure[p["closure"]]
-        b = D.SplineBuilder(bs, None, c, c, tile_lines=2, chunks=int(min(max(n // 16, 2), 256)))
+        b = D.SplineBuilder(bs, None, c, c, tile_lines=2, chunks=int(min(max(n // 16, 2), 256)), precision=precision,
+                            refine_rounds=refine_rounds)
         e = D.SplineEvaluator(bs)
         nlo = b.s_nbv_xmin if c == 1 else 0
         nhi = b.s_nbv_xmax if c == 1 else 0

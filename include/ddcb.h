@@ -236,15 +236,21 @@ ddcb_status ddcb_build_eval_adjoint(ddcb_builder b, ddcb_evaluator e, int32_t or
 /* ---- uneven batch: many independent one-line problems (each its own builder and evaluator:
  *      size, degree, closure and mesh may all differ) built and evaluated by persistent kernels
  *      in one CUDA graph launch (no reference counterpart: the reference loops one SplineBuilder
- *      per problem). The builders and evaluators must outlive the batch and use FP64. Data are
- *      packed: problem i's samples at vals[vals_off[i] .. vals_off[i+1]), its Hermite
- *      derivatives likewise in derivs_lo / derivs_hi, its coefficients in coefs, and its
- *      evaluation coordinates / values in coords / out at [evals_off[i] .. evals_off[i+1]). */
+ *      per problem). The builders and evaluators must outlive the batch; each solves in its own
+ *      precision (FP64, or FP32 with refinement, whose convergence ddcb_builder_device_status
+ *      reports per builder). Data are packed: problem i's samples at
+ *      vals[vals_off[i] .. vals_off[i+1]), its Hermite derivatives likewise in derivs_lo /
+ *      derivs_hi, its coefficients in coefs, and its evaluation coordinates / values in coords /
+ *      out at [evals_off[i] .. evals_off[i+1]). */
 typedef struct ddcb_uneven_batch_t* ddcb_uneven_batch;
 typedef struct ddcb_uneven_info {
     int64_t count, total_vals, total_derivs_lo, total_derivs_hi, total_coefs, total_evals;
-    int32_t threads, blocks_per_sm, order, shared_bytes; /* the schedule in use (order 0: largest first) */
-    double tuned_us;                                     /* the tuner's best time (0: not tuned) */
+    /* the schedule in use: threads = block size of the block schedule; blocks_per_sm = per-SM
+     * budget in units of 256 threads (0: as many blocks as fit); order 0: largest first */
+    int32_t threads, blocks_per_sm, order, shared_bytes;
+    double tuned_us;       /* the tuner's best time (0: not tuned) */
+    int32_t warp_schedule; /* 1: each problem's block has one thread per chunk of its plan, whole
+                              warps (a warp per problem of <= 32 chunks); 0: every block `threads` */
 } ddcb_uneven_info;
 ddcb_status ddcb_batch_uneven_create(const ddcb_builder* builders, const ddcb_evaluator* evaluators,
                                      const int64_t* nevals, int64_t count, ddcb_uneven_batch* out);
@@ -253,8 +259,9 @@ ddcb_status ddcb_batch_uneven_get_info(ddcb_uneven_batch b, ddcb_uneven_info* in
 /* Prefix sums (count + 1 entries each; any pointer may be NULL). */
 ddcb_status ddcb_batch_uneven_offsets(ddcb_uneven_batch b, int64_t* vals_off, int64_t* derivs_lo_off,
                                       int64_t* derivs_hi_off, int64_t* coefs_off, int64_t* evals_off);
-/* Times the candidate schedules (block size, blocks per SM, queue order), `reps` launches each, on
- * these buffers and keeps the fastest for later runs. Overwrites coefs and out. */
+/* Times the candidate schedules (warp or block schedule, block size, per-SM budget, queue order),
+ * `reps` launches each, on these buffers and keeps the fastest for later runs. Overwrites coefs and
+ * out. */
 ddcb_status ddcb_batch_uneven_tune(ddcb_uneven_batch b, const double* vals, const double* derivs_lo,
                                    const double* derivs_hi, double* coefs, const double* coords, double* out,
                                    int32_t reps, ddcb_stream stream);
@@ -312,12 +319,14 @@ ddcb_status ddcb_build2d(ddcb_builder b1, ddcb_builder b2, double* coefs, const 
  * framework that owns all device memory), which also cannot hand over a workspace.
  * Same arguments and results as ddcb_build2d with workspace == NULL, but the scratch of the x1 pass
  * is a fixed array of 48 MiB (50331648 bytes) inside the library's device image, present on every
- * GPU that loads the library until the process exits. Requests whose ddcb_build2d_workspace_bytes
- * exceed it are rejected with DDCB_ERR_UNSUPPORTED. The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress, once per device); make that first call before
- * any stream capture. All calls share the one array: calls whose work overlaps on the GPU (other
- * streams, other host threads) race on it and must be ordered by the caller. The scratch needs no
- * clearing: every value is written before it is read. */
+ * GPU that loads the library until the process exits. The fields run in groups small enough for
+ * the array; a build whose scratch exceeds it even with one field per group is rejected with
+ * DDCB_ERR_UNSUPPORTED. The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress, once per device, kept for the life of the process: a device reset
+ * between calls is not supported); make that first call before any stream capture (a first call
+ * under capture is refused with DDCB_ERR_INVALID_ARGUMENT). All calls share the one array: calls
+ * whose work overlaps on the GPU (other streams, other host threads) race on it and must be
+ * ordered by the caller. The scratch needs no clearing: every value is written before it is read. */
 ddcb_status ddcb_build2d_static_scratch(ddcb_builder b1, ddcb_builder b2, double* coefs, const double* vals,
                                         const double* derivs_min1, const double* derivs_max1, const double* derivs_min2,
                                         const double* derivs_max2, const double* mixed_min1_min2,

@@ -1,7 +1,8 @@
 """The uneven batch (ddcb_batch_uneven_*): one graph launch of persistent kernels over problems of
 different size, degree, closure and mesh, against the per-problem builder + evaluator calls (the
-same arithmetic, so the results must be identical) and against the oracle on a sample (<= 1e-12,
-or 10*cond(A)*eps for the ill-conditioned systems)."""
+same arithmetic, so the results must be identical) and against the oracle on every problem (<= 1e-12,
+or 10*cond(A)*eps for the ill-conditioned systems), in FP64 and in FP32 with FP64 refinement, under
+the warp and the block schedules."""
 import numpy as np
 import pytest
 
@@ -10,14 +11,14 @@ torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module")
-def setup():
+@pytest.fixture(scope="module", params=["fp64", "fp32_refine"])
+def setup(request):
     import ddc_b200 as D
     from ddc_b200 import workloads as W
 
     D.load_library()
     probs = W.config4(count=257, nmax=1500, seed=0xDDC0 + 44)
-    w = W.config4_batch(D, probs)
+    w = W.config4_batch(D, probs, precision=request.param)
     batch = D.UnevenBatch(w["builders"], w["evaluators"], w["nevals"])
     cu = lambda a: torch.from_numpy(a).cuda()
     dev = dict(vals=cu(w["vals"]), dlo=cu(w["dlo"]), dhi=cu(w["dhi"]), coords=cu(w["coords"]))
@@ -67,20 +68,22 @@ def test_graph_replay_and_tuning_keep_results(setup):
     c1, o1 = run(batch, dev)
     c2, o2 = run(batch, dev)  # replays the cached graph
     info = batch.tune(dev["vals"], dev["dlo"], dev["dhi"], dev["coefs"], dev["coords"], dev["out"], reps=1)
-    assert info.tuned_us > 0 and info.threads in (128, 256, 512)
+    assert info.tuned_us > 0 and info.threads in (128, 256, 512) and info.warp_schedule in (0, 1)
     c3, o3 = run(batch, dev)  # the graph of the tuned schedule
     for c, o in ((c2, o2), (c3, o3)):
         np.testing.assert_array_equal(c, c1)
         np.testing.assert_array_equal(o, o1)
+    for b in w["builders"]:
+        b.device_status()  # refined problems converged (FP64 ones never flag)
 
 
-def test_batch_against_oracle_sample(setup, oracle_mod):
+def test_batch_against_oracle_every_problem(setup, oracle_mod):
     O = oracle_mod
     D, W, probs, w, batch, dev = setup
     off = batch.offsets()
     coefs, out = run(batch, dev)
     clos = {"periodic": O.PERIODIC, "hermite": O.HERMITE, "greville": O.GREVILLE}
-    for i in range(0, len(probs), 16):
+    for i in range(len(probs)):
         p, b = probs[i], w["builders"][i]
         per = p["closure"] == "periodic"
         obs = (O.BSplines(p["degree"], per, rmin=0.0, rmax=1.0, ncells=p["ncells"]) if p["uniform"]

@@ -24,3 +24,19 @@ def test_device_solve_emulation(tmp_path):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-3000:]
     assert "0 failures" in r.stdout
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_plan_matrix_equals_reference_matrix(tmp_path, oracle_mod):
+    """tests/native/matrix_check.cpp: the plan's assembled system equals the oracle's restatement of
+    the reference's matrix (including the symmetric storage of uniform centre blocks) entry by
+    entry, for degrees 1-5, uniform and non-uniform, every closure pair and sizes 7..429."""
+    exe = str(tmp_path / "matrix_check")
+    obuild = os.path.join(ROOT, "oracle", "_build")
+    cmd = ["g++", "-std=c++17", "-O1", "-Wno-subobject-linkage", "-I/usr/local/cuda/include", "-x", "c++",
+           os.path.join(ROOT, "tests", "native", "matrix_check.cpp"), "-x", "none", f"-L{obuild}", "-loracle",
+           f"-Wl,-rpath,{obuild}", "-L/usr/local/cuda/lib64", "-lcudart", "-o", exe]
+    subprocess.run(cmd, check=True, capture_output=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-3000:]
+    assert "0 failures" in r.stdout
