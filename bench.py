@@ -521,7 +521,8 @@ def measure_configs(peak, reps):
     ws3 = torch.empty(bld3.workspace_bytes(F) // 8 + 1, dtype=torch.float64, device=dev)
     tb3 = _time_ms(lambda i: bld3(c3, v3, workspace=ws3, derivs_min2=dm, derivs_max2=dM), reps)
     ev3 = D.SplineEvaluator3D(*[D.SplineEvaluator(bb) for bb in b3])
-    x3 = torch.rand((np3[0] * np3[1] * np3[2] // 4, F, 3), dtype=torch.float64, device=dev)
+    # evaluation points shared by the fields (as the feet of an advection step are)
+    x3 = torch.rand((np3[0] * np3[1] * np3[2] // 4, 1, 3), dtype=torch.float64, device=dev).expand(-1, F, 3).contiguous()
     y3 = torch.empty((x3.shape[0], F), dtype=torch.float64, device=dev)
     te3 = _time_ms(lambda i: ev3(y3, x3, c3), reps)
     bb3 = (v3.numel() + dm.numel() + dM.numel() + c3.numel()) * 8

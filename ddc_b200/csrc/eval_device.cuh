@@ -274,6 +274,26 @@ __device__ __forceinline__ double nonuniform_deriv1(EvalBasis const& eb, double 
     return y;
 }
 
+// s'(x) on a non-uniform basis from the derivative spline's coefficients: Acc holds
+// d_j = D (c_j - c_{j-1}) / (t_{j+D} - t_j), the coefficients of s' on the degree-(D-1) B-splines
+// (de Boor, "A Practical Guide to Splines", X.(15)), so a point needs the 2(D-1) knots around its
+// cell and the degree-(D-1) basis only: no divided-difference factors, one knot pair fewer than
+// nonuniform_deriv1. D >= 2.
+template <int D, class Acc>
+__device__ __forceinline__ double nonuniform_deriv1_dcoef(EvalBasis const& eb, double x, Acc const& C)
+{
+    constexpr int P = D - 1;
+    double kn[2 * P]; // t[ck-P+1 .. ck+P]
+    int const ck = locate_load_knots<P>(eb, x, kn);
+    double v[P + 1];
+    nonuniform_values_div<P>(kn, x, v);
+    int const r0 = C.row0(ck - P);
+    double y = 0.0;
+#pragma unroll
+    for (int r = 0; r < P + 1; ++r) y = fma(C.get(r0, r), v[r], y);
+    return y;
+}
+
 // s(x) without boundary handling (spline_evaluator.hpp:556-605).
 template <int D, bool UNI, class Acc>
 __device__ __forceinline__ double eval_value_no_bc(EvalBasis const& eb, double x, Acc const& C)

@@ -65,6 +65,10 @@ __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const __grid_constan
     int const nct = blockDim.x / TLE;
     int64_t const line = (int64_t)blockIdx.x * TLE + l;
     bool const live = line < a.nlines;
+    // First derivatives on non-uniform bases evaluate the derivative spline: once the tile is in,
+    // it is turned into d_j = D (c_j - c_{j-1}) / (t_{j+D} - t_j) (row 0 unused), once per line
+    // instead of once per point (below).
+    constexpr bool DSPLINE = !UNI && ORDER == 1 && D >= 2;
     if (a.pair16) {
         // two lines per 16-byte copy (cp.async.cg bypasses L1, where the basis tables live)
         int const p = tid % (TLE / 2);
@@ -89,6 +93,24 @@ __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const __grid_constan
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
+    if (DSPLINE) {
+        // in place: each thread owns a contiguous run of rows of its line, keeps the row before the
+        // run, and converts the run from its end (c_{j-1} is read before d_{j-1} replaces it)
+        int const per = (a.size + nct - 1) / nct;
+        int const r0 = c * per, r1 = min(a.size, r0 + per);
+        double const before = (live && r0 > 0 && r0 < a.size) ? C[(r0 - 1) * TLE + l] : 0.0;
+        __syncthreads();
+        if (live && r0 < r1) {
+            const double* g = a.eb.inv_span + (size_t)(D - 1) * a.eb.nk; // 1/(t_{j+D} - t_j) at g[j]
+            double cj = C[(r1 - 1) * TLE + l];
+            for (int j = r1 - 1; j >= r0; --j) {
+                double const cprev = j > r0 ? C[(j - 1) * TLE + l] : before;
+                C[j * TLE + l] = j > 0 ? double(D) * (cj - cprev) * __ldg(g + j) : 0.0;
+                cj = cprev;
+            }
+        }
+        __syncthreads();
+    }
     if (!live) return;
     EvalBasis eb = a.eb;
     if (!UNI) {
@@ -109,8 +131,13 @@ __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const __grid_constan
 #pragma unroll
         for (int u = 0; u < U; ++u) xs[u] = (q0 + u < npt) ? __ldcs(xp + (q0 + u) * sx) : 0.0;
 #pragma unroll
-        for (int u = 0; u < U; ++u)
-            if (q0 + u < npt) __stcs(op + (q0 + u) * so, eval_point<D, ORDER, UNI>(eb, a.ex_lo, a.ex_hi, xs[u], acc));
+        for (int u = 0; u < U; ++u) {
+            if (q0 + u >= npt) continue;
+            double y;
+            if constexpr (DSPLINE) y = nonuniform_deriv1_dcoef<D>(eb, xs[u], acc);
+            else y = eval_point<D, ORDER, UNI>(eb, a.ex_lo, a.ex_hi, xs[u], acc);
+            __stcs(op + (q0 + u) * so, y);
+        }
     }
 }
 

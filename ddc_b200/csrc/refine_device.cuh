@@ -39,9 +39,10 @@ __device__ __forceinline__ void residual_tile(BuildArgs const& args, const doubl
 
 // The convergence check of the refined lines, from the last correction d (no extra residual
 // pass): the solve that produced d works in FP32 on an FP32-rounded residual, so the refined X
-// carries an error of about cond(A) (2^-24 max|d| + 2^-52 max|X|); a line whose bound, with a
-// factor 4, exceeds refine_tol * max|X| sets bit 0 of the builder's status word (read by
-// ddcb_builder_device_status). dmax / xmax: this thread's maxima of its line (threads own one line
+// carries an error of at most about cond(A) 2^-24 max|d| beyond the FP64 rounding every solve
+// has; a line whose bound, with a factor 4, exceeds refine_tol * max|X| sets bit 0 of the
+// builder's status word (read by ddcb_builder_device_status). The bound is a worst case: one
+// round rarely certifies a system with cond(A) above a few tens, two rounds usually do. dmax / xmax: this thread's maxima of its line (threads own one line
 // each in the accumulation loops); `red`: 2 TL shared 8-byte words. Ends with a barrier.
 template <int TL>
 __device__ __forceinline__ void convergence_check(BuildArgs const& args, double dmax, double xmax, unsigned long long* red)
@@ -57,7 +58,7 @@ __device__ __forceinline__ void convergence_check(BuildArgs const& args, double 
     if (threadIdx.x < TL && tile_line0<TL>(args) + threadIdx.x < args.nlines) {
         double const d = __longlong_as_double(static_cast<long long>(red[threadIdx.x]));
         double const x = __longlong_as_double(static_cast<long long>(red[TL + threadIdx.x]));
-        double const bound = 4.0 * t.cond_est * (0x1p-24 * d + 0x1p-52 * x);
+        double const bound = 4.0 * t.cond_est * 0x1p-24 * d;
         if (!(bound <= t.refine_tol * x)) atomicOr(t.status, 1u);
     }
     __syncthreads();

