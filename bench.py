@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--no-configs", action="store_true", help="skip the other configurations' measurements")
     p.add_argument("--cpu-stub", action="store_true",
                    help="CPU ranks (gloo) with a NumPy step in place of the GPU kernels: checks the rank logic only")
-    p.add_argument("--profile-case", choices=["adjoint", "periodic_cubic", "tensor2d"], default=None,
+    p.add_argument("--profile-case", choices=["adjoint", "periodic_cubic", "tensor2d", "uneven", "quintic"], default=None,
                    help="run only this case's kernels, --steps times on --lines lines (for profilers; prints no JSON line)")
     return p.parse_args()
 
@@ -699,7 +699,8 @@ def profile_case(args):
     """A short run of one case's kernels at a chosen batch, for ncu captures on small workloads:
     adjoint = periodic cubic 1024 cells, build + evaluate then its backward; periodic_cubic = the
     fused build + evaluate of 1000 cells; tensor2d = the 2D build and evaluation of 512 x 512 cells
-    over --lines fields."""
+    over --lines fields; uneven = the 4096-problem uneven batch (untuned schedule); quintic = the
+    headline's builder and first-derivative evaluator on --lines lines."""
     import torch
 
     import ddc_b200 as D
@@ -722,6 +723,29 @@ def profile_case(args):
             b.build_and_evaluate(e, c, v, x, y)
             if args.profile_case == "adjoint":
                 b.build_and_evaluate_adjoint(e, x, c, g, gv, gx)
+    elif args.profile_case == "uneven":
+        probs = W.config4()
+        wb = W.config4_batch(D, probs)
+        batch = D.UnevenBatch(wb["builders"], wb["evaluators"], wb["nevals"])
+        info = batch.info
+        cu = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        bv, blo, bhi, bx = cu(wb["vals"]), cu(wb["dlo"]), cu(wb["dhi"]), cu(wb["coords"])
+        bc = torch.empty((info.total_coefs,), dtype=torch.float64, device=dev)
+        by = torch.empty((info.total_evals,), dtype=torch.float64, device=dev)
+        for _ in range(args.steps):
+            batch(bv, blo, bhi, bc, bx, by)
+    elif args.profile_case == "quintic":
+        bs, pts, br = workload_plan(D, B)
+        builder = D.SplineBuilder(bs, pts, D.SplineBuilderClosure.HERMITE, D.SplineBuilderClosure.HERMITE)
+        ev = D.SplineEvaluator(bs)
+        w = make_inputs(pts, B, 1024)
+        cu = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        vals, dlo, dhi, x = cu(w["vals"]), cu(w["dlo"]), cu(w["dhi"]), cu(w["coords"])
+        coefs = torch.empty((bs.size, B), dtype=torch.float64, device=dev)
+        out = torch.empty((1024, B), dtype=torch.float64, device=dev)
+        for _ in range(args.steps):
+            builder(coefs, vals, dlo, dhi)
+            ev.deriv(1, out, x, coefs)
     else:
         w = W.config3(nfields=B)
         cu = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)

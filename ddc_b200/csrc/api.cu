@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -18,6 +19,8 @@ struct ddcb_bsplines_t
 struct ddcb_builder_t
 {
     ddcb::Builder* b;
+    std::mutex quad_mutex;    // guards the first computation of the quadrature weights
+    bool quad_ready = false;
 };
 struct ddcb_evaluator_t
 {
@@ -288,19 +291,21 @@ ddcb_status ddcb_builder_create(ddcb_bsplines basis, const double* interp_points
             delete h;
             throw;
         }
-        try {
-            // the quadrature weights, by the device transposed solve
-            ddcb::compute_device_quadrature(*h->b, h->b->d_quad_scratch, h->b->d_quad);
-        } catch (...) {
-            ddcb::destroy_builder(h->b);
-            delete h;
-            throw;
-        }
         *out = h;
     });
 }
 
 static void check_device(int device, char const* what);
+
+// The quadrature weights of a builder, computed on its first use (device transposed solve and
+// builder adjoint, synchronous), once.
+static void ensure_quadrature(ddcb_builder h)
+{
+    std::lock_guard<std::mutex> lock(h->quad_mutex);
+    if (h->quad_ready) return;
+    ddcb::compute_device_quadrature(*h->b, h->b->d_quad_scratch, h->b->d_quad);
+    h->quad_ready = true;
+}
 
 ddcb_status ddcb_builder_device_status(ddcb_builder h, ddcb_stream stream)
 {
@@ -485,6 +490,7 @@ ddcb_status ddcb_quadrature_coefficients(ddcb_builder h, double* qlo, double* q,
         require(b.nbv_lo == 0 || qlo != nullptr, "q_derivs_lo is NULL");
         require(b.nbv_hi == 0 || qhi != nullptr, "q_derivs_hi is NULL");
         check_device(b.device, "builder");
+        ensure_quadrature(h);
         std::vector<double> all(size_t(b.n));
         DDCB_CUDA_CHECK(cudaMemcpy(all.data(), b.d_quad, sizeof(double) * all.size(), cudaMemcpyDeviceToHost));
         long const nv = b.n - b.nbv_lo - b.nbv_hi;
@@ -501,6 +507,7 @@ ddcb_status ddcb_quadrature_coefficients_device(ddcb_builder h, double* q_all, d
         require(q_all != nullptr, "q_all is NULL");
         ddcb::Builder const& b = *h->b;
         check_device(b.device, "builder");
+        ensure_quadrature(h);
         DDCB_CUDA_CHECK(cudaMemcpyAsync(q_all, b.d_quad, sizeof(double) * size_t(b.n), cudaMemcpyDeviceToDevice,
                                         reinterpret_cast<cudaStream_t>(stream)));
     });
@@ -530,6 +537,7 @@ ddcb_status ddcb_integrate_samples(ddcb_builder h, double* out, int64_t out_oute
             check_lines(lhi, b.nbv_hi, "derivs_hi");
             same_batch(lv, lhi, "derivs_hi");
         }
+        ensure_quadrature(h);
         ddcb::launch_integrate_samples(b, out, out_outer_stride, vals, ddcb::to_lines(lv), her_lo ? dlo : nullptr,
                                        ddcb::to_lines(llo), her_hi ? dhi : nullptr, ddcb::to_lines(lhi),
                                        reinterpret_cast<cudaStream_t>(stream));

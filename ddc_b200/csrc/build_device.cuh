@@ -16,6 +16,8 @@
 // splines_linear_problem_2x2_blocks.cpp:274-298) applied in shared memory.
 #pragma once
 
+#include <type_traits>
+
 #include "ddcb_internal.hpp"
 
 namespace ddcb {
@@ -79,6 +81,15 @@ __device__ __forceinline__ double2 add2(double2 a, double2 b) { return make_doub
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 sub2(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// the same on a single line (a tile of one line: no partner)
+__device__ __forceinline__ double fma2(double a, double y, double w) { return fma(a, y, w); }
+__device__ __forceinline__ float fma2(float a, float y, float w) { return fmaf(a, y, w); }
+__device__ __forceinline__ double mul2(double v, double d) { return v * d; }
+__device__ __forceinline__ float mul2(float v, float d) { return v * d; }
+__device__ __forceinline__ double add2(double a, double b) { return a + b; }
+__device__ __forceinline__ float add2(float a, float b) { return a + b; }
+__device__ __forceinline__ double sub2(double a, double b) { return a - b; }
+__device__ __forceinline__ float sub2(float a, float b) { return a - b; }
 
 // The factor tables in the arithmetic type R of a solve: the FP64 tables, or their FP32 copies
 // (the FP32 solves of the refinement mode).
@@ -111,23 +122,29 @@ struct Fac<float>
     __device__ static const float* Qg(SolveTables const& t) { return t.f32.Qg; }
 };
 
+// What a thread's chunk works on: a pair of lines (V = Fac<R>::V, 2 lanes), or the one line of a
+// single-line tile (V = R).
+template <class R, int TL>
+using Lanes = typename std::conditional<TL % 2 == 0, typename Fac<R>::V, R>::type;
+template <class V>
+__device__ __forceinline__ V zero_of() { return V {}; }
+
 // Forward sweep with L (and the row interchanges when PIV) over rows [a, e) (chunk c) of a line
-// pair; T2 points at the pair's column (row j at T2[j*P]). w[0..KL-1] hold rows a..a+KL-1 on
+// pair (or of the single line); T2 points at the pair's column (row j at T2[j*P]). w[0..KL-1] hold rows a..a+KL-1 on
 // entry. Phase A (WRITE false) reads rows beyond e from the tile, which nothing has written yet.
 // Phase C (WRITE true) writes rows a..e-1; without interchanges rows beyond e only feed the next
 // chunk's rows, so they are not read; with interchanges they come from the halo copy.
-template <class R, int KL, bool PIV, bool WRITE, int UNR>
-__device__ __forceinline__ void fwd_sweep(SolveTables const& t, typename Fac<R>::V* T2, int P, int a, int e, int c,
-                                          typename Fac<R>::V* w, const typename Fac<R>::V* halo, int hstride)
+template <class R, class V, int KL, bool PIV, bool WRITE, int UNR>
+__device__ __forceinline__ void fwd_sweep(SolveTables const& t, V* T2, int P, int a, int e, int c, V* w, const V* halo,
+                                          int hstride)
 {
-    using V = typename Fac<R>::V;
     R const* __restrict__ Lf = Fac<R>::Lf(t);
     int const lim = (WRITE && !PIV) ? e : t.m; // fill rows below lim are read
     int const qs = factor_stride(t);
 #pragma unroll UNR
     for (int j = a; j < e; ++j) {
         int const rr = j + KL;
-        V fill = Fac<R>::zero();
+        V fill = zero_of<V>();
         if (rr < e) fill = T2[rr * P];
         else if (rr < lim) fill = (WRITE && PIV) ? halo[(rr - e) * hstride] : T2[rr * P];
         w[KL] = fill;
@@ -153,11 +170,9 @@ __device__ __forceinline__ void fwd_sweep(SolveTables const& t, typename Fac<R>:
 
 // Backward sweep with U over rows e-1 .. a (chunk c) of a line pair; z[0..KU-1] hold the solution
 // rows e .. e+KU-1 (the carry from the chunk below) on entry.
-template <class R, int KU, bool WRITE, int UNR>
-__device__ __forceinline__ void bwd_sweep(SolveTables const& t, typename Fac<R>::V* T2, int P, int a, int e, int c,
-                                          typename Fac<R>::V* z)
+template <class R, class V, int KU, bool WRITE, int UNR>
+__device__ __forceinline__ void bwd_sweep(SolveTables const& t, V* T2, int P, int a, int e, int c, V* z)
 {
-    using V = typename Fac<R>::V;
     R const* __restrict__ Uf = Fac<R>::Uf(t);
     int const qs = factor_stride(t);
 #pragma unroll UNR
@@ -180,11 +195,9 @@ __device__ __forceinline__ void bwd_sweep(SolveTables const& t, typename Fac<R>:
 // out(c) = Phi_c out(c-1) + hat(c); step k adds P(k,c) y(c-2^k). Backward: the carry flows from
 // c+1 into c with Q(k,c) y(c+2^k). Every thread of the block takes part in the barriers; threads
 // of chunk c < NC do the arithmetic.
-template <class R, int K, int KC, bool FWD>
-__device__ __forceinline__ void carry_scan(const R* __restrict__ Pm, typename Fac<R>::V* C2, int P, int nscan, int NC,
-                                           int c)
+template <class R, class V, int K, int KC, bool FWD, bool PRE_OK = true>
+__device__ __forceinline__ void carry_scan(const R* __restrict__ Pm, V* C2, int P, int nscan, int NC, int c)
 {
-    using V = typename Fac<R>::V;
     V y[K];
     bool const act = c < NC;
     if (act) {
@@ -195,8 +208,9 @@ __device__ __forceinline__ void carry_scan(const R* __restrict__ Pm, typename Fa
         int const nb = FWD ? c - (1 << k) : c + (1 << k);
         bool const has = act && (FWD ? nb >= 0 : nb < NC);
         V v[K];
-        // the matrix is read before the barrier (its loads overlap the wait) when it is small
-        constexpr bool PRE = K <= 4;
+        // the matrix is read before the barrier (its loads overlap the wait) when it is small and
+        // the caller can spare the registers
+        constexpr bool PRE = PRE_OK && K <= 4;
         R mk[PRE ? K * K : 1];
         if (has) {
             if constexpr (PRE) {
@@ -249,16 +263,18 @@ inline int fit_tile_lines(int TL, Bytes bytes)
 // Steps 2-4 of a solve on a tile already in shared memory (T[j*TL + l] = right-hand side row j of
 // line l, in the arithmetic type R): forward and backward sweeps, border correction. A thread owns
 // one chunk of a pair of lines (paired shared-memory accesses; each factor load serves both
-// lines). The carries, halo and border scratch follow the n rows (tile_doubles elements of R in
-// all). On return (after a barrier) T holds the solution. Every thread of the block must call it;
-// TL is even and the block has at least nchunk * TL / 2 threads.
-// UNR0 (0: the default) sets the rows unrolled per sweep step.
-template <int TL, int KL, int KU, class R = double, int UNR0 = 0>
+// lines), or of the one line of a TL = 1 tile. The carries, halo and border scratch follow the n
+// rows (tile_doubles elements of R in all). On return (after a barrier) T holds the solution.
+// Every thread of the block must call it; TL is even or 1, and the block has at least
+// nchunk * max(TL / 2, 1) threads.
+// UNR0 (0: the default) sets the rows unrolled per sweep step; PRE lets the carry scans load their
+// transfer matrices before each barrier (K x K registers more).
+template <int TL, int KL, int KU, class R = double, int UNR0 = 0, bool PRE = true>
 __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/, R* smem)
 {
-    static_assert(TL % 2 == 0, "the solve works on line pairs");
-    using V = typename Fac<R>::V;
-    constexpr int P = TL / 2;
+    static_assert(TL % 2 == 0 || TL == 1, "the solve works on line pairs, or on one line");
+    using V = Lanes<R, TL>;
+    constexpr int P = TL % 2 == 0 ? TL / 2 : 1;
     constexpr int KC = KL > KU ? KL : KU;
     // rows unrolled per sweep step: 4 by default; a single line pair is not unrolled, which keeps
     // its kernels free of spills
@@ -273,7 +289,7 @@ __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/,
     V* const carry = T2 + (size_t)n * P;                 // NC x KC rows
     V* const halo = carry + (size_t)NC * KC * P;         // NC x KL rows (row interchanges only)
     V* const btmp = halo + (t.pivot ? (size_t)NC * KL * P : 0); // k rows
-    V const zero = Fac<R>::zero();
+    V const zero = zero_of<V>();
 
     int a = 0, e = 0;
     if (c < NC) {
@@ -287,8 +303,8 @@ __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/,
             V w[KL + 1];
 #pragma unroll
             for (int q = 0; q < KL; ++q) w[q] = (a + q < m) ? T2[(a + q) * P] : zero;
-            if (t.pivot) fwd_sweep<R, KL, true, false, UNR>(t, T2, P, a, e, c, w, nullptr, 0);
-            else fwd_sweep<R, KL, false, false, UNR>(t, T2, P, a, e, c, w, nullptr, 0);
+            if (t.pivot) fwd_sweep<R, V, KL, true, false, UNR>(t, T2, P, a, e, c, w, nullptr, 0);
+            else fwd_sweep<R, V, KL, false, false, UNR>(t, T2, P, a, e, c, w, nullptr, 0);
 #pragma unroll
             for (int q = 0; q < KL; ++q) {
                 V const orig = (e + q < m) ? T2[(e + q) * P] : zero;
@@ -297,7 +313,7 @@ __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/,
             }
         }
         __syncthreads();
-        carry_scan<R, KL, KC, true>(Fac<R>::PhiF(t), carry, P, t.nscan_f, NC, c);
+        carry_scan<R, V, KL, KC, true, PRE>(Fac<R>::PhiF(t), carry, P, t.nscan_f, NC, c);
         if (c < NC) {
             V w[KL + 1];
 #pragma unroll
@@ -306,8 +322,8 @@ __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/,
                 if (c > 0 && a + q < m) v = add2(v, carry[((c - 1) * KC + q) * P]);
                 w[q] = v;
             }
-            if (t.pivot) fwd_sweep<R, KL, true, true, UNR>(t, T2, P, a, e, c, w, halo + (size_t)c * KL * P, P);
-            else fwd_sweep<R, KL, false, true, UNR>(t, T2, P, a, e, c, w, nullptr, 0);
+            if (t.pivot) fwd_sweep<R, V, KL, true, true, UNR>(t, T2, P, a, e, c, w, halo + (size_t)c * KL * P, P);
+            else fwd_sweep<R, V, KL, false, true, UNR>(t, T2, P, a, e, c, w, nullptr, 0);
         }
         __syncthreads();
 
@@ -316,17 +332,17 @@ __device__ __forceinline__ void solve_in_tile(SolveTables const& t, int /*nct*/,
             V z[KU];
 #pragma unroll
             for (int q = 0; q < KU; ++q) z[q] = zero;
-            bwd_sweep<R, KU, false, UNR>(t, T2, P, a, e, c, z);
+            bwd_sweep<R, V, KU, false, UNR>(t, T2, P, a, e, c, z);
 #pragma unroll
             for (int q = 0; q < KU; ++q) carry[(c * KC + q) * P] = z[q];
         }
         __syncthreads();
-        carry_scan<R, KU, KC, false>(Fac<R>::PhiB(t), carry, P, t.nscan_b, NC, c);
+        carry_scan<R, V, KU, KC, false, PRE>(Fac<R>::PhiB(t), carry, P, t.nscan_b, NC, c);
         if (c < NC) {
             V z[KU];
 #pragma unroll
             for (int q = 0; q < KU; ++q) z[q] = (c + 1 < NC) ? carry[((c + 1) * KC + q) * P] : zero;
-            bwd_sweep<R, KU, true, UNR>(t, T2, P, a, e, c, z);
+            bwd_sweep<R, V, KU, true, UNR>(t, T2, P, a, e, c, z);
         }
         __syncthreads();
     }
@@ -400,8 +416,9 @@ __device__ __forceinline__ void gather_tile(BuildArgs const& args, double* T)
     if (TL % 2 == 0 && args.pair16) {
         // two adjacent lines per 16-byte copy, which bypasses L1 (cp.async.cg) and so leaves the
         // solve tables resident there
-        int const p = tid % (TL / 2);
-        int const c2 = tid / (TL / 2);
+        constexpr int HP = TL / 2 > 0 ? TL / 2 : 1; // line pairs of the tile (TL even here)
+        int const p = tid % HP;
+        int const c2 = tid / HP;
         int64_t const line = tile_line0<TL>(args) + 2 * p;
         bool const live0 = line < args.nlines, live1 = line + 1 < args.nlines;
         int64_t const ov = live0 ? line_offset(args.lv, line) : 0;
@@ -467,8 +484,9 @@ __device__ __forceinline__ void store_tile(BuildArgs const& args, const double* 
     int const tid = threadIdx.x;
     int const rows = args.raw ? n : args.r.size;
     if (TL % 2 == 0 && args.pair16_out) {
-        int const p = tid % (TL / 2);
-        int const c2 = tid / (TL / 2);
+        constexpr int HP = TL / 2 > 0 ? TL / 2 : 1; // line pairs of the tile (TL even here)
+        int const p = tid % HP;
+        int const c2 = tid / HP;
         int64_t const line = tile_line0<TL>(args) + 2 * p;
         if (line >= args.nlines) return;
         int64_t const oo = line_offset(args.lo, line);

@@ -194,6 +194,21 @@ __device__ __forceinline__ void nonuniform_values_span2(const double* kn, const 
     }
 }
 
+// 1/d for a positive normal d: the hardware approximation (rcp.approx.ftz.f64) refined by two
+// Newton-Raphson steps r <- r + r (1 - d r) (quadratic convergence: the approximation's ~20 bits
+// become more than the 53 of a double; within an ulp or two of the rounded quotient), without the
+// special-case path of an IEEE division. Used for knot differences, which are positive and far from
+// the range limits.
+__device__ __forceinline__ double recip_newton(double d)
+{
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+    double e = fma(-d, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-d, r, 1.0);
+    return fma(r, e, r);
+}
+
 // Non-uniform Cox-de Boor values of degree P on the cell whose knots are kn (the layout of
 // nonuniform_values_span), dividing by the knot differences themselves: the j+1 denominators of
 // level j are inverted together with one division (prefix products, then one reciprocal, then
@@ -217,7 +232,7 @@ __device__ __forceinline__ void nonuniform_values_div(const double* kn, double x
             d[r] = den;
             pre[r] = r == 0 ? d[0] : pre[r - 1] * d[r];
         }
-        double inv = 1.0 / pre[j];
+        double inv = recip_newton(pre[j]);
 #pragma unroll
         for (int r = j; r >= 1; --r) {
             inv_d[r] = inv * pre[r - 1];

@@ -4,8 +4,8 @@
 // SplineBuilder::quadrature_coefficients (spline_builder.hpp:1103-1234) solves A^T q = I, with I_j
 // the integral of B-spline j (integrals.hpp), so that the integral of the spline built from a
 // right-hand side f is I . A^-1 f = q . f. Here the transposed solve is the device kernel of the
-// multi-right-hand-side solve (in place, on one column), run once when the builder is created;
-// the weights stay on the device.
+// multi-right-hand-side solve (in place, on one column), run once, on the builder's first use of
+// its weights; the weights stay on the device.
 //
 // The reference takes I in basis order without the periodic column offset of the builder
 // (spline_builder.hpp:619-658, 1061-1100), so on non-uniform periodic bases with a non-zero offset

@@ -1,5 +1,5 @@
 // uneven_batch.cu -- thousands of independent 1D spline problems of different size, degree,
-// closure and mesh, built and evaluated by persistent kernels in ONE graph launch.
+// closure and mesh, built and evaluated in ONE graph launch.
 //
 // Each problem is one line: a builder (its device factor tables) and an evaluator, with its
 // samples, derivatives, coefficients, coordinates and values packed one after another in flat
@@ -8,13 +8,19 @@
 // FP64 refinement), and by block size: under the warp schedule a problem's block has one thread
 // per chunk of its plan, rounded up to a warp, so short problems (<= 32 chunks) run one warp each,
 // many per SM, with barriers that cost a warp's; under the block schedule every block has
-// `threads` threads. Each group gets a persistent kernel with a fixed grid (its share, by work, of a
-// per-SM thread budget); every block takes the group's next problem from a counter (largest-first
-// order by default, so the long problems start early and the short ones fill the tail), builds it
-// in shared memory with the chunked tile solve of the batched builder (the chunks' carries chained
-// by the log-depth scan across the block's threads), stores its coefficients and evaluates its
-// points from the solved tile. The per-problem description is copied into shared memory once per
-// problem, so the solve reads its tables' addresses from there.
+// `threads` threads. A problem is a tile of ONE line: the chunk threads sweep scalar rows (no
+// empty partner line), so a problem's shared memory is its n rows plus the chunk carries.
+//
+// Each group gets a build kernel whose grid holds, by default, one block per problem (block b
+// starts with queue position b; with a smaller grid, later problems come from a counter, in
+// largest-first order by default). A block copies its problem's description into shared memory,
+// gathers the right-hand side, runs the chunked tile solve of the batched builder (the chunks'
+// carries chained by the log-depth scan across the block's threads) and stores the coefficients.
+// Each group's evaluation kernel, which depends on that group's build kernel only, evaluates the
+// group's points from the stored coefficients with 256-thread blocks over segments of 512 points,
+// so the points of a problem are spread over many threads instead of waiting on its chunk
+// threads, and the short problems' evaluations overlap the long problems' builds. The build
+// kernels of the groups with the longest problems get the highest stream priorities.
 //
 // ddcb_batch_uneven_run launches a CUDA graph holding the counter reset and the group kernels,
 // which run concurrently; the graph is rebuilt only when the buffers, stream or schedule change.
@@ -38,13 +44,19 @@ static int const kNumShapes = int(sizeof(kShapes) / sizeof(kShapes[0]));
 struct UnevenProblem
 {
     BuildArgs args;        // data pointers hold offsets into the packed arrays (added at run time)
-    EvalBasis eb;
-    int ex_lo, ex_hi;
     int shape;             // index into kShapes
     int rounds;            // refinement rounds (FP32 solve); -1: FP64 solve
+};
+
+// What the evaluation of one problem needs.
+struct UnevenEval
+{
+    EvalBasis eb;
+    int ex_lo, ex_hi;
     int degree, uniform;
     int m;                 // evaluation points
-    int64_t x_off, out_off;
+    int64_t x_off;         // first coordinate (and output value) in the packed arrays
+    int64_t coef_off;      // first coefficient in the packed array
 };
 
 struct UnevenArgs
@@ -57,46 +69,51 @@ struct UnevenArgs
     const double* dlo;
     const double* dhi;
     double* coefs;
+};
+
+// A block's share of one problem's points: kSegment points from `first` on (fewer at the end).
+struct UnevenSegment
+{
+    int prob;
+    int first;
+    int64_t x;             // packed index of its first coordinate and value
+};
+
+struct UnevenEvalArgs
+{
+    const UnevenEval* evals;
+    const UnevenSegment* segs;
+    const double* coefs;
     const double* coords;
     double* out;
 };
 
+// Sweep rows unrolled per step (their factor loads issue together) and no transfer-matrix loads
+// ahead of the scan barriers (registers for more resident problems): measured on the uneven
+// workload of 4096 problems.
+constexpr int kUnevenUnroll = 4;
+constexpr bool kUnevenScanPrefetch = false;
+constexpr int kEvalThreads = 256;
+constexpr int kEvalPts = 2;                           // points per thread
+constexpr int kSegment = kEvalThreads * kEvalPts;     // points per evaluation block
+
 namespace {
 
-template <int D, bool UNI>
-__device__ __noinline__ void eval_line(EvalBasis const& eb, int ex_lo, int ex_hi, CoefRotated const& acc,
-                                       const double* __restrict__ x, double* __restrict__ out, int m)
-{
-    for (int q = threadIdx.x; q < m; q += blockDim.x) __stcs(out + q, eval_point<D, 0, UNI>(eb, ex_lo, ex_hi, __ldcs(x + q), acc));
-}
-
-__device__ __forceinline__ void eval_any(int degree, int uniform, EvalBasis const& eb, int ex_lo, int ex_hi,
-                                         CoefRotated const& acc, const double* x, double* out, int m)
-{
-    switch (degree * 2 + uniform) {
-    case 2: eval_line<1, false>(eb, ex_lo, ex_hi, acc, x, out, m); break;
-    case 3: eval_line<1, true>(eb, ex_lo, ex_hi, acc, x, out, m); break;
-    case 4: eval_line<2, false>(eb, ex_lo, ex_hi, acc, x, out, m); break;
-    case 5: eval_line<2, true>(eb, ex_lo, ex_hi, acc, x, out, m); break;
-    case 6: eval_line<3, false>(eb, ex_lo, ex_hi, acc, x, out, m); break;
-    case 7: eval_line<3, true>(eb, ex_lo, ex_hi, acc, x, out, m); break;
-    case 8: eval_line<4, false>(eb, ex_lo, ex_hi, acc, x, out, m); break;
-    case 9: eval_line<4, true>(eb, ex_lo, ex_hi, acc, x, out, m); break;
-    case 10: eval_line<5, false>(eb, ex_lo, ex_hi, acc, x, out, m); break;
-    default: eval_line<5, true>(eb, ex_lo, ex_hi, acc, x, out, m); break;
-    }
-}
-
+// Narrow bands fit in 64 registers (two 512-thread blocks per SM), so the one-warp blocks of short
+// problems pack 32 to an SM; wider bands keep the registers that spare them spills.
 template <int KL, int KU, bool REFINE>
-__global__ void __launch_bounds__(512) uneven_kernel(const __grid_constant__ UnevenArgs A)
+__global__ void __launch_bounds__(512, (KL + KU <= (REFINE ? 3 : 4) ? 2 : 1)) uneven_build_kernel(const __grid_constant__ UnevenArgs A)
 {
     extern __shared__ __align__(16) double smem[];
     __shared__ UnevenProblem sp;
     __shared__ int s_next;
-    for (;;) {
-        if (threadIdx.x == 0) s_next = atomicAdd(A.counter, 1);
-        __syncthreads();
-        int const qi = s_next;
+    // the first problem of block b is queue position b; later ones come from the counter
+    for (int pass = 0;; ++pass) {
+        if (pass > 0) {
+            if (threadIdx.x == 0) s_next = int(gridDim.x) + atomicAdd(A.counter, 1);
+            __syncthreads();
+        }
+        int const qi = pass > 0 ? s_next : int(blockIdx.x);
         if (qi >= A.nprob) break;
         // the problem's description into shared memory, offsets turned into pointers
         {
@@ -110,19 +127,68 @@ __global__ void __launch_bounds__(512) uneven_kernel(const __grid_constant__ Une
             sp.args.dlo = A.dlo + reinterpret_cast<intptr_t>(sp.args.dlo);
             sp.args.dhi = A.dhi + reinterpret_cast<intptr_t>(sp.args.dhi);
             sp.args.out = A.coefs + reinterpret_cast<intptr_t>(sp.args.out);
-            sp.args.nct = blockDim.x / 2;
+            sp.args.nct = blockDim.x;
         }
         __syncthreads();
         if constexpr (REFINE) {
-            refine_tile<2, KL, KU>(sp.args, smem, sp.rounds);
+            refine_tile<1, KL, KU>(sp.args, smem, sp.rounds);
         } else {
-            gather_tile<2>(sp.args, smem);
-            solve_in_tile<2, KL, KU>(sp.args.t, 0, smem);
+            gather_tile<1>(sp.args, smem);
+            solve_in_tile<1, KL, KU, double, kUnevenUnroll, kUnevenScanPrefetch>(sp.args.t, 0, smem);
         }
-        store_tile<2>(sp.args, smem);
-        CoefRotated const acc {smem, 2, sp.args.t.n, sp.args.r.srot};
-        eval_any(sp.degree, sp.uniform, sp.eb, sp.ex_lo, sp.ex_hi, acc, A.coords + sp.x_off, A.out + sp.out_off, sp.m);
+        store_tile<1>(sp.args, smem);
         __syncthreads(); // the tile and the description are reused by the next problem
+    }
+}
+
+// The thread's points of a segment (q0 + k * kEvalThreads, k < kEvalPts): coordinates loaded
+// first, so the evaluations' load chains overlap.
+template <int D, bool UNI>
+__device__ __forceinline__ void eval_seg(UnevenEval const& e, double const* coefs, double const* xv, double* y, int live)
+{
+    CoefGlobal const acc {coefs + e.coef_off, 1};
+#pragma unroll
+    for (int k = 0; k < kEvalPts; ++k)
+        if (k < live) __stcs(y + k * kEvalThreads, eval_point<D, 0, UNI>(e.eb, e.ex_lo, e.ex_hi, xv[k], acc));
+}
+
+// One block per segment of a problem's points (kEvalPts per thread); the coefficients come from
+// the build kernels (the graph orders them before this kernel).
+__global__ void __launch_bounds__(kEvalThreads, 4) uneven_eval_kernel(const __grid_constant__ UnevenEvalArgs A)
+{
+    __shared__ UnevenEval se;
+    UnevenSegment const seg = A.segs[blockIdx.x];
+    // the description and this thread's coordinates load together
+    {
+        const int* src = reinterpret_cast<const int*>(A.evals + seg.prob);
+        int* dst = reinterpret_cast<int*>(&se);
+        for (int i = threadIdx.x; i < int(sizeof(UnevenEval) / sizeof(int)); i += blockDim.x) dst[i] = __ldg(src + i);
+    }
+    double xv[kEvalPts];
+    int live = 0;
+    {
+        int const m = __ldg(&A.evals[seg.prob].m);
+#pragma unroll
+        for (int k = 0; k < kEvalPts; ++k) {
+            int const q = seg.first + int(threadIdx.x) + k * kEvalThreads;
+            xv[k] = q < m ? __ldcs(A.coords + seg.x + threadIdx.x + k * kEvalThreads) : 0.0;
+            live += q < m ? 1 : 0;
+        }
+    }
+    __syncthreads();
+    if (live == 0) return;
+    double* y = A.out + seg.x + threadIdx.x;
+    switch (se.degree * 2 + se.uniform) {
+    case 2: eval_seg<1, false>(se, A.coefs, xv, y, live); break;
+    case 3: eval_seg<1, true>(se, A.coefs, xv, y, live); break;
+    case 4: eval_seg<2, false>(se, A.coefs, xv, y, live); break;
+    case 5: eval_seg<2, true>(se, A.coefs, xv, y, live); break;
+    case 6: eval_seg<3, false>(se, A.coefs, xv, y, live); break;
+    case 7: eval_seg<3, true>(se, A.coefs, xv, y, live); break;
+    case 8: eval_seg<4, false>(se, A.coefs, xv, y, live); break;
+    case 9: eval_seg<4, true>(se, A.coefs, xv, y, live); break;
+    case 10: eval_seg<5, false>(se, A.coefs, xv, y, live); break;
+    default: eval_seg<5, true>(se, A.coefs, xv, y, live); break;
     }
 }
 
@@ -132,17 +198,17 @@ template <bool R>
 UnevenKernel kernel_of_r(int shape)
 {
     switch (shape) {
-    case 0: return uneven_kernel<1, 1, R>;
-    case 1: return uneven_kernel<1, 2, R>;
-    case 2: return uneven_kernel<2, 2, R>;
-    case 3: return uneven_kernel<3, 3, R>;
-    case 4: return uneven_kernel<1, 4, R>;
-    case 5: return uneven_kernel<2, 4, R>;
-    case 6: return uneven_kernel<4, 4, R>;
-    case 7: return uneven_kernel<3, 6, R>;
-    case 8: return uneven_kernel<1, 8, R>;
-    case 9: return uneven_kernel<2, 8, R>;
-    default: return uneven_kernel<4, 8, R>;
+    case 0: return uneven_build_kernel<1, 1, R>;
+    case 1: return uneven_build_kernel<1, 2, R>;
+    case 2: return uneven_build_kernel<2, 2, R>;
+    case 3: return uneven_build_kernel<3, 3, R>;
+    case 4: return uneven_build_kernel<1, 4, R>;
+    case 5: return uneven_build_kernel<2, 4, R>;
+    case 6: return uneven_build_kernel<4, 4, R>;
+    case 7: return uneven_build_kernel<3, 6, R>;
+    case 8: return uneven_build_kernel<1, 8, R>;
+    case 9: return uneven_build_kernel<2, 8, R>;
+    default: return uneven_build_kernel<4, 8, R>;
     }
 }
 
@@ -151,7 +217,7 @@ UnevenKernel kernel_of(int shape, bool refine) { return refine ? kernel_of_r<tru
 size_t problem_smem(UnevenProblem const& p)
 {
     int const kl = kShapes[p.shape][0], ku = kShapes[p.shape][1];
-    return p.rounds >= 0 ? refine_smem(p.args.t, 2, kl, ku) : sizeof(double) * tile_doubles(p.args.t, 2, kl, ku);
+    return p.rounds >= 0 ? refine_smem(p.args.t, 1, kl, ku) : sizeof(double) * tile_doubles(p.args.t, 1, kl, ku);
 }
 
 // The block of a problem under the warp schedule: one thread per chunk, whole warps.
@@ -165,11 +231,17 @@ struct UnevenBatch
     int64_t count = 0;
     std::vector<int64_t> vals_off, dlo_off, dhi_off, coef_off, x_off; // count + 1 prefix sums
     UnevenProblem* d_probs = nullptr;
+    UnevenEval* d_evals = nullptr;
+    UnevenSegment* d_segs = nullptr; // evaluation segments
+    int64_t nseg = 0;
     // per group (band shape, arithmetic, warp-schedule block size): its problems in two queue
     // orders (largest-first, then natural) at d_order + 2*gfirst[g] and d_order + 2*gfirst[g] +
     // gsize[g]; its counter d_counter[g]
     std::vector<int> gshape, grefine, gclass, gfirst, gsize;
-    std::vector<double> gcost;
+    std::vector<int64_t> gseg0, gnseg;  // the group's evaluation segments in d_segs
+    std::vector<double> gcost, gmax;  // per group: total and largest problem cost
+    std::vector<int> grank;           // groups ranked by their largest problem (0: the largest)
+    int nrank = 1;
     std::vector<size_t> gsmem;
     int* d_order = nullptr;
     int* d_counter = nullptr;
@@ -180,11 +252,14 @@ struct UnevenBatch
     int threads = 256;
     int blocks_per_sm = 0;     // per-SM budget in units of 256 threads (0: as many blocks as fit)
     int order = 0;             // 0 largest-first, 1 natural
+    int prio = 1;              // 1: the groups' kernels get priorities by their largest problem
     double tuned_us = 0.0;
     // cached graph
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     UnevenArgs key {};
+    const double* key_coords = nullptr;
+    double* key_out = nullptr;
     cudaStream_t key_stream = nullptr;
     int key_threads = 0, key_blocks = 0, key_order = -1, key_warp = -1;
 };
@@ -206,8 +281,8 @@ int group_threads(UnevenBatch const& b, int g)
     return b.warp ? c : std::max(b.threads, c);
 }
 
-// Blocks of group g's kernel: its share (by work) of the per-SM budget (blocks_per_sm x 256
-// threads; 0: as many blocks as fit) over the SMs, at least one, at most its problem count.
+// Blocks of group g's kernel: the per-SM budget (blocks_per_sm x 256 threads; 0: as many blocks
+// as fit) over the SMs, at least one, at most its problem count.
 int group_blocks(UnevenBatch const& b, int g, int threads, int per_sm)
 {
     UnevenKernel k = kernel_of(b.gshape[size_t(g)], b.grefine[size_t(g)] != 0);
@@ -216,16 +291,16 @@ int group_blocks(UnevenBatch const& b, int g, int threads, int per_sm)
     int fit = 0;
     DDCB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k, threads, sm));
     if (fit < 1) throw Error(DDCB_ERR_UNSUPPORTED, "the largest problem's tile does not fit in shared memory");
+    // every group may start all its problems at once: its grid is capped by its problem count and
+    // by the blocks that fit (or the budget); the groups' kernels share the GPU concurrently, and
+    // blocks that do not fit yet queue behind the running ones
     int const per = per_sm > 0 ? std::min(std::max(1, per_sm * 256 / threads), fit) : fit;
-    double total = 0.0;
-    for (double c : b.gcost) total += c;
-    double const share = total > 0.0 ? b.gcost[size_t(g)] / total : 1.0;
-    int64_t const blocks = std::llround(share * per * sm_count());
+    int64_t const blocks = int64_t(per) * sm_count();
     return int(std::max<int64_t>(1, std::min<int64_t>(blocks, b.gsize[size_t(g)])));
 }
 
 UnevenArgs make_args(UnevenBatch const& b, int g, int order, double const* vals, double const* dlo, double const* dhi,
-                     double* coefs, double const* coords, double* out)
+                     double* coefs)
 {
     UnevenArgs a {};
     a.probs = b.d_probs;
@@ -236,8 +311,6 @@ UnevenArgs make_args(UnevenBatch const& b, int g, int order, double const* vals,
     a.dlo = dlo;
     a.dhi = dhi;
     a.coefs = coefs;
-    a.coords = coords;
-    a.out = out;
     return a;
 }
 
@@ -259,6 +332,8 @@ UnevenBatch* create_uneven_batch(Builder const* const* builders, Evaluator const
         DDCB_CUDA_CHECK(cudaGetDevice(&b->device));
         b->count = count;
         std::vector<UnevenProblem> probs(static_cast<size_t>(count));
+        std::vector<UnevenEval> evs(static_cast<size_t>(count));
+        std::vector<UnevenSegment> segs;
         b->vals_off.assign(size_t(count) + 1, 0);
         b->dlo_off = b->dhi_off = b->coef_off = b->x_off = b->vals_off;
         std::vector<double> cost(static_cast<size_t>(count));
@@ -300,19 +375,20 @@ UnevenBatch* create_uneven_batch(Builder const* const* builders, Evaluator const
             a.lo = Lines {size, 1, 1, 1, 0};
             a.pair16 = a.pair16_out = 0;
             a.line_base = 0; // one line per problem, its arrays already offset
-            p.eb = ev.eb;
-            p.ex_lo = ev.ex_lo;
-            p.ex_hi = ev.ex_hi;
-            p.degree = ev.basis.desc.degree;
-            p.uniform = ev.basis.desc.uniform ? 1 : 0;
-            p.m = int(nevals[i]);
-            p.x_off = b->x_off[i];
-            p.out_off = b->x_off[i];
+            UnevenEval& e = evs[size_t(i)];
+            e.eb = ev.eb;
+            e.ex_lo = ev.ex_lo;
+            e.ex_hi = ev.ex_hi;
+            e.degree = ev.basis.desc.degree;
+            e.uniform = ev.basis.desc.uniform ? 1 : 0;
+            e.m = int(nevals[i]);
+            e.x_off = b->x_off[i];
+            e.coef_off = b->coef_off[i];
             b->max_chunks = std::max(b->max_chunks, bl.tables.nchunk);
             // a block's time on a problem: a fixed part (barriers, scans, the description) plus
-            // the rows and points its threads step through
+            // the rows its threads step through
             cost[size_t(i)] = 64.0 + double(np) * (kShapes[p.shape][0] + kShapes[p.shape][1] + 2) / 8.0
-                              + double(nevals[i]) * (p.degree + 1) / 8.0;
+                              ;
         }
         // groups by band shape, arithmetic and warp-schedule block size (the tile of a group is
         // sized to its largest problem); queue orders within each group
@@ -322,13 +398,14 @@ UnevenBatch* create_uneven_batch(Builder const* const* builders, Evaluator const
                 for (int cls = 32; cls <= 512; cls += 32) {
                     std::vector<int> members;
                     size_t smem = 0;
-                    double c = 0.0;
+                    double c = 0.0, cmax = 0.0;
                     for (int64_t i = 0; i < count; ++i) {
                         UnevenProblem const& p = probs[size_t(i)];
                         if (p.shape != sh || (p.rounds >= 0) != (rf == 1) || warp_class(p.args.t.nchunk) != cls) continue;
                         members.push_back(int(i));
                         smem = std::max(smem, problem_smem(p));
                         c += cost[size_t(i)];
+                        cmax = std::max(cmax, cost[size_t(i)]);
                     }
                     if (members.empty()) continue;
                     b->gshape.push_back(sh);
@@ -337,12 +414,20 @@ UnevenBatch* create_uneven_batch(Builder const* const* builders, Evaluator const
                     b->gfirst.push_back(int(order.size() / 2));
                     b->gsize.push_back(int(members.size()));
                     b->gcost.push_back(c);
+                    b->gmax.push_back(cmax);
                     b->gsmem.push_back((smem + 15) & ~size_t(15));
                     b->smem = std::max(b->smem, b->gsmem.back());
                     std::vector<int> lpt = members;
                     std::stable_sort(lpt.begin(), lpt.end(), [&](int x, int y) { return cost[size_t(x)] > cost[size_t(y)]; });
                     order.insert(order.end(), lpt.begin(), lpt.end());
                     order.insert(order.end(), members.begin(), members.end());
+                    // the group's evaluation segments, largest problems first
+                    b->gseg0.push_back(int64_t(segs.size()));
+                    for (int i : lpt) {
+                        UnevenEval const& e = evs[size_t(i)];
+                        for (int q0 = 0; q0 < e.m; q0 += kSegment) segs.push_back(UnevenSegment {i, q0, e.x_off + q0});
+                    }
+                    b->gnseg.push_back(int64_t(segs.size()) - b->gseg0.back());
                 }
             }
         }
@@ -351,6 +436,22 @@ UnevenBatch* create_uneven_batch(Builder const* const* builders, Evaluator const
             DDCB_CUDA_CHECK(cudaMemcpy(b->d_probs, probs.data(), sizeof(UnevenProblem) * size_t(count), cudaMemcpyHostToDevice));
             DDCB_CUDA_CHECK(cudaMalloc(&b->d_order, sizeof(int) * order.size()));
             DDCB_CUDA_CHECK(cudaMemcpy(b->d_order, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice));
+            DDCB_CUDA_CHECK(cudaMalloc(&b->d_evals, sizeof(UnevenEval) * size_t(count)));
+            DDCB_CUDA_CHECK(cudaMemcpy(b->d_evals, evs.data(), sizeof(UnevenEval) * size_t(count), cudaMemcpyHostToDevice));
+        }
+        {
+            std::vector<int> idx(b->gmax.size());
+            std::iota(idx.begin(), idx.end(), 0);
+            std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return b->gmax[size_t(x)] > b->gmax[size_t(y)]; });
+            b->grank.assign(idx.size(), 0);
+            for (size_t r = 0; r < idx.size(); ++r) b->grank[size_t(idx[r])] = int(r);
+            b->nrank = std::max<int>(1, int(idx.size()));
+        }
+        if (segs.size() >= size_t(1) << 31) throw Error(DDCB_ERR_UNSUPPORTED, "more than 2^31 evaluation segments");
+        b->nseg = int64_t(segs.size());
+        if (b->nseg > 0) {
+            DDCB_CUDA_CHECK(cudaMalloc(&b->d_segs, sizeof(UnevenSegment) * segs.size()));
+            DDCB_CUDA_CHECK(cudaMemcpy(b->d_segs, segs.data(), sizeof(UnevenSegment) * segs.size(), cudaMemcpyHostToDevice));
         }
         DDCB_CUDA_CHECK(cudaMalloc(&b->d_counter, sizeof(int) * std::max<size_t>(1, b->gshape.size())));
         b->threads = std::max(256, (b->max_chunks + 31) / 32 * 32);
@@ -366,6 +467,8 @@ void destroy_uneven_batch(UnevenBatch* b)
     if (!b) return;
     drop_graph(*b);
     if (b->d_probs) cudaFree(b->d_probs);
+    if (b->d_evals) cudaFree(b->d_evals);
+    if (b->d_segs) cudaFree(b->d_segs);
     if (b->d_order) cudaFree(b->d_order);
     if (b->d_counter) cudaFree(b->d_counter);
     delete b;
@@ -403,9 +506,9 @@ void run_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, dou
                       double const* coords, double* out, cudaStream_t s)
 {
     if (b.count == 0) return;
-    UnevenArgs const key = make_args(b, 0, b.order, vals, dlo, dhi, coefs, coords, out);
+    UnevenArgs const key = make_args(b, 0, b.order, vals, dlo, dhi, coefs);
     bool const stale = !b.exec || key.vals != b.key.vals || key.dlo != b.key.dlo || key.dhi != b.key.dhi
-                       || key.coefs != b.key.coefs || key.coords != b.key.coords || key.out != b.key.out
+                       || key.coefs != b.key.coefs || coords != b.key_coords || out != b.key_out
                        || s != b.key_stream || b.threads != b.key_threads || b.blocks_per_sm != b.key_blocks
                        || b.order != b.key_order || b.warp != b.key_warp;
     if (stale) {
@@ -420,8 +523,13 @@ void run_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, dou
         mp.pitch = 0;
         cudaGraphNode_t mnode = nullptr;
         DDCB_CUDA_CHECK(cudaGraphAddMemsetNode(&mnode, b.graph, nullptr, 0, &mp));
+        // the groups of the longest problems first in the block scheduler's eye: their kernels
+        // get the higher priorities, so their blocks are not queued behind the short problems'
+        int least = 0, greatest = 0;
+        DDCB_CUDA_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        std::vector<cudaGraphNode_t> built;
         for (int g = 0; g < int(b.gshape.size()); ++g) {
-            UnevenArgs args = make_args(b, g, b.order, vals, dlo, dhi, coefs, coords, out);
+            UnevenArgs args = make_args(b, g, b.order, vals, dlo, dhi, coefs);
             void* params[] = {&args};
             cudaKernelNodeParams kp {};
             int const th = group_threads(b, g);
@@ -432,9 +540,33 @@ void run_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, dou
             kp.kernelParams = params;
             cudaGraphNode_t knode = nullptr;
             DDCB_CUDA_CHECK(cudaGraphAddKernelNode(&knode, b.graph, &mnode, 1, &kp));
+            if (b.prio && greatest != least) {
+                cudaLaunchAttributeValue v {};
+                // numerically lower is higher: the largest group gets `greatest`, the smallest `least`
+                v.priority = std::min(least, greatest + b.grank[size_t(g)] * (least - greatest) / std::max(1, b.nrank - 1));
+                DDCB_CUDA_CHECK(cudaGraphKernelNodeSetAttribute(knode, cudaLaunchAttributePriority, &v));
+            }
+            built.push_back(knode);
+        }
+        // each group's points are evaluated once its own problems are built, while the other
+        // groups may still be building
+        for (int g = 0; g < int(b.gshape.size()); ++g) {
+            if (b.gnseg[size_t(g)] == 0) continue;
+            UnevenEvalArgs ea {b.d_evals, b.d_segs + b.gseg0[size_t(g)], coefs, coords, out};
+            void* params[] = {&ea};
+            cudaKernelNodeParams kp {};
+            kp.func = reinterpret_cast<void*>(uneven_eval_kernel);
+            kp.gridDim = dim3(unsigned(b.gnseg[size_t(g)]));
+            kp.blockDim = dim3(unsigned(kEvalThreads));
+            kp.sharedMemBytes = 0;
+            kp.kernelParams = params;
+            cudaGraphNode_t enode = nullptr;
+            DDCB_CUDA_CHECK(cudaGraphAddKernelNode(&enode, b.graph, &built[size_t(g)], 1, &kp));
         }
         DDCB_CUDA_CHECK(cudaGraphInstantiate(&b.exec, b.graph, 0));
         b.key = key;
+        b.key_coords = coords;
+        b.key_out = out;
         b.key_stream = s;
         b.key_threads = b.threads;
         b.key_blocks = b.blocks_per_sm;
@@ -463,7 +595,7 @@ void tune_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, do
             int warp, threads, per;
         };
         std::vector<Cand> cands;
-        for (int per : {2, 4, 6, 8}) cands.push_back({1, 256, per});
+        for (int per : {0, 1, 2, 4, 8}) cands.push_back({1, 256, per});
         for (int threads : {128, 256, 512})
             for (int per : {1, 2, 4, 8}) cands.push_back({0, threads, per});
         for (Cand const& cd : cands) {

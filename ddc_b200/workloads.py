@@ -148,9 +148,11 @@ def config4_samples(p, points, nbv_lo, nbv_hi):
 
 def config4_batch(D, probs, precision="fp64", refine_rounds=2):
     """Builders, evaluators and packed host inputs (flat arrays in problem order) of config4
-    problems; `D` is the ddc_b200 package. Each builder solves one line: tile width 2 and about 16
-    rows per chunk (so problems under 512 rows have at most 32 chunks: one warp each under the warp
-    schedule). precision "fp32_refine" builds every problem in FP32 with FP64 refinement."""
+    problems; `D` is the ddc_b200 package. Each builder solves one line, cut into whole warps of
+    chunks: ceil(rows / 512) warps of 32 chunks (at most 16 rows per chunk; problems under 512
+    rows take one warp, with chunks as short as the band allows), so no thread of a problem's
+    block idles and the chunk sweeps are as short as the warp count permits. precision
+    "fp32_refine" builds every problem in FP32 with FP64 refinement."""
     closure = {"periodic": 0, "hermite": 1, "greville": 3}
     builders, evaluators, nevals = [], [], []
     vals, dlo, dhi, coords = [], [], [], []
@@ -159,7 +161,8 @@ def config4_batch(D, probs, precision="fp64", refine_rounds=2):
         per = p["closure"] == "periodic"
         bs = D.UniformBSplines(d, per, 0.0, 1.0, n) if p["uniform"] else D.NonUniformBSplines(d, per, p["breaks"])
         c = closure[p["closure"]]
-        b = D.SplineBuilder(bs, None, c, c, tile_lines=2, chunks=int(min(max(n // 16, 2), 256)), precision=precision,
+        chunks = 32 * max(1, -(-bs.size // 512))
+        b = D.SplineBuilder(bs, None, c, c, tile_lines=2, chunks=int(min(chunks, 512)), precision=precision,
                             refine_rounds=refine_rounds)
         e = D.SplineEvaluator(bs)
         nlo = b.s_nbv_xmin if c == 1 else 0

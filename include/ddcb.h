@@ -145,8 +145,9 @@ ddcb_status ddcb_solve_multirhs(ddcb_builder b, double* rhs, int64_t ld, int64_t
                                 ddcb_stream stream);
 /* SplineBuilder::quadrature_coefficients() (spline_builder.hpp:1103-1234), host outputs of
  * nbv_lo, nbasis - nbv_lo - nbv_hi and nbv_hi entries; the Hermite parts are scaled by dx^k. The
- * weights solve A^T q = integrals with the device's transposed solve, once, when the builder is
- * created; this call copies them out (synchronously). */
+ * weights solve A^T q = integrals with the device's transposed solve, on the builder's first
+ * quadrature or ddcb_integrate_samples call (synchronously, once); this call copies them out
+ * (synchronously). */
 ddcb_status ddcb_quadrature_coefficients(ddcb_builder b, double* q_derivs_lo, double* q_vals, double* q_derivs_hi);
 /* The same weights as one device array of nbasis entries, [q_derivs_lo, q_vals, q_derivs_hi],
  * copied stream-ordered into q_all (a device pointer): quadrature_coefficients<OutMemorySpace>()
