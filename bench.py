@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--no-configs", action="store_true", help="skip the other configurations' measurements")
     p.add_argument("--cpu-stub", action="store_true",
                    help="CPU ranks (gloo) with a NumPy step in place of the GPU kernels: checks the rank logic only")
-    p.add_argument("--profile-case", choices=["adjoint", "periodic_cubic", "tensor2d", "uneven", "quintic"], default=None,
+    p.add_argument("--profile-case", choices=["adjoint", "periodic_cubic", "tensor2d", "uneven", "quintic", "quintic_refine"], default=None,
                    help="run only this case's kernels, --steps times on --lines lines (for profilers; prints no JSON line)")
     return p.parse_args()
 
@@ -700,7 +700,8 @@ def profile_case(args):
     adjoint = periodic cubic 1024 cells, build + evaluate then its backward; periodic_cubic = the
     fused build + evaluate of 1000 cells; tensor2d = the 2D build and evaluation of 512 x 512 cells
     over --lines fields; uneven = the 4096-problem uneven batch (untuned schedule); quintic = the
-    headline's builder and first-derivative evaluator on --lines lines."""
+    headline's builder and first-derivative evaluator on --lines lines; quintic_refine = its
+    builder in FP32 with one FP64 refinement round."""
     import torch
 
     import ddc_b200 as D
@@ -734,9 +735,11 @@ def profile_case(args):
         by = torch.empty((info.total_evals,), dtype=torch.float64, device=dev)
         for _ in range(args.steps):
             batch(bv, blo, bhi, bc, bx, by)
-    elif args.profile_case == "quintic":
+    elif args.profile_case in ("quintic", "quintic_refine"):
         bs, pts, br = workload_plan(D, B)
-        builder = D.SplineBuilder(bs, pts, D.SplineBuilderClosure.HERMITE, D.SplineBuilderClosure.HERMITE)
+        prec = "fp32_refine" if args.profile_case == "quintic_refine" else "fp64"
+        builder = D.SplineBuilder(bs, pts, D.SplineBuilderClosure.HERMITE, D.SplineBuilderClosure.HERMITE,
+                                  precision=prec, refine_rounds=1)
         ev = D.SplineEvaluator(bs)
         w = make_inputs(pts, B, 1024)
         cu = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)

@@ -99,10 +99,8 @@ constexpr int kSegment = kEvalThreads * kEvalPts;     // points per evaluation b
 
 namespace {
 
-// Narrow bands fit in 64 registers (two 512-thread blocks per SM), so the one-warp blocks of short
-// problems pack 32 to an SM; wider bands keep the registers that spare them spills.
 template <int KL, int KU, bool REFINE>
-__global__ void __launch_bounds__(512, (KL + KU <= (REFINE ? 3 : 4) ? 2 : 1)) uneven_build_kernel(const __grid_constant__ UnevenArgs A)
+__global__ void __launch_bounds__(512, 1) uneven_build_kernel(const __grid_constant__ UnevenArgs A)
 {
     extern __shared__ __align__(16) double smem[];
     __shared__ UnevenProblem sp;
@@ -130,11 +128,16 @@ __global__ void __launch_bounds__(512, (KL + KU <= (REFINE ? 3 : 4) ? 2 : 1)) un
             sp.args.nct = blockDim.x;
         }
         __syncthreads();
+        // register copies of the tables: read from shared memory, their addresses would have to be
+        // reloaded after every store to the tile (the compiler cannot rule out aliasing), which
+        // serialises the sweeps' factor loads row by row
         if constexpr (REFINE) {
-            refine_tile<1, KL, KU>(sp.args, smem, sp.rounds);
+            BuildArgs const args = sp.args;
+            refine_tile<1, KL, KU>(args, smem, sp.rounds);
         } else {
             gather_tile<1>(sp.args, smem);
-            solve_in_tile<1, KL, KU, double, kUnevenUnroll, kUnevenScanPrefetch>(sp.args.t, 0, smem);
+            SolveTables const t = sp.args.t;
+            solve_in_tile<1, KL, KU, double, kUnevenUnroll, kUnevenScanPrefetch>(t, 0, smem);
         }
         store_tile<1>(sp.args, smem);
         __syncthreads(); // the tile and the description are reused by the next problem
@@ -524,11 +527,15 @@ void run_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, dou
         cudaGraphNode_t mnode = nullptr;
         DDCB_CUDA_CHECK(cudaGraphAddMemsetNode(&mnode, b.graph, nullptr, 0, &mp));
         // the groups of the longest problems first in the block scheduler's eye: their kernels
-        // get the higher priorities, so their blocks are not queued behind the short problems'
+        // are added first and get the higher priorities (the graph is instantiated to use node
+        // priorities), so their blocks are not queued behind the short problems'
         int least = 0, greatest = 0;
         DDCB_CUDA_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-        std::vector<cudaGraphNode_t> built;
-        for (int g = 0; g < int(b.gshape.size()); ++g) {
+        int const ng = int(b.gshape.size());
+        std::vector<int> by_rank(size_t(ng), 0);
+        for (int g = 0; g < ng; ++g) by_rank[size_t(b.grank[size_t(g)])] = g;
+        std::vector<cudaGraphNode_t> built(size_t(ng), nullptr);
+        for (int g : by_rank) {
             UnevenArgs args = make_args(b, g, b.order, vals, dlo, dhi, coefs);
             void* params[] = {&args};
             cudaKernelNodeParams kp {};
@@ -546,11 +553,11 @@ void run_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, dou
                 v.priority = std::min(least, greatest + b.grank[size_t(g)] * (least - greatest) / std::max(1, b.nrank - 1));
                 DDCB_CUDA_CHECK(cudaGraphKernelNodeSetAttribute(knode, cudaLaunchAttributePriority, &v));
             }
-            built.push_back(knode);
+            built[size_t(g)] = knode;
         }
         // each group's points are evaluated once its own problems are built, while the other
         // groups may still be building
-        for (int g = 0; g < int(b.gshape.size()); ++g) {
+        for (int g : by_rank) {
             if (b.gnseg[size_t(g)] == 0) continue;
             UnevenEvalArgs ea {b.d_evals, b.d_segs + b.gseg0[size_t(g)], coefs, coords, out};
             void* params[] = {&ea};
@@ -563,7 +570,7 @@ void run_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, dou
             cudaGraphNode_t enode = nullptr;
             DDCB_CUDA_CHECK(cudaGraphAddKernelNode(&enode, b.graph, &built[size_t(g)], 1, &kp));
         }
-        DDCB_CUDA_CHECK(cudaGraphInstantiate(&b.exec, b.graph, 0));
+        DDCB_CUDA_CHECK(cudaGraphInstantiateWithFlags(&b.exec, b.graph, b.prio ? cudaGraphInstantiateFlagUseNodePriority : 0));
         b.key = key;
         b.key_coords = coords;
         b.key_out = out;
