@@ -19,6 +19,7 @@ def setup(request):
     D.load_library()
     probs = W.config4(count=257, nmax=1500, seed=0xDDC0 + 44)
     w = W.config4_batch(D, probs, precision=request.param)
+    w["precision"] = request.param
     batch = D.UnevenBatch(w["builders"], w["evaluators"], w["nevals"])
     cu = lambda a: torch.from_numpy(a).cuda()
     dev = dict(vals=cu(w["vals"]), dlo=cu(w["dlo"]), dhi=cu(w["dhi"]), coords=cu(w["coords"]))
@@ -83,6 +84,7 @@ def test_batch_against_oracle_every_problem(setup, oracle_mod):
     off = batch.offsets()
     coefs, out = run(batch, dev)
     clos = {"periodic": O.PERIODIC, "hermite": O.HERMITE, "greville": O.GREVILLE}
+    worst_c = worst_y = 0.0
     for i in range(len(probs)):
         p, b = probs[i], w["builders"][i]
         per = p["closure"] == "periodic"
@@ -100,7 +102,13 @@ def test_batch_against_oracle_every_problem(setup, oracle_mod):
         assert np.abs(got - ref).max() <= tol * np.abs(ref).max(), (i, p["ncells"], p["degree"], p["closure"])
         x = w["coords"][off["evals"][i]:off["evals"][i + 1]]
         ev = O.evaluate(obs, x[:, None], ref[:, None])[:, 0]
-        assert np.abs(out[off["evals"][i]:off["evals"][i + 1]] - ev).max() <= tol * max(np.abs(ev).max(), 1e-300)
+        # values relative to max(|values|, |coefficients|): the B-splines sum to one, so a value's
+        # error is at most the largest coefficient error
+        scale = max(np.abs(ev).max(), np.abs(ref).max())
+        assert np.abs(out[off["evals"][i]:off["evals"][i + 1]] - ev).max() <= tol * scale
+        worst_c = max(worst_c, np.abs(got - ref).max() / np.abs(ref).max())
+        worst_y = max(worst_y, np.abs(out[off["evals"][i]:off["evals"][i + 1]] - ev).max() / scale)
+    print(f"PARITY uneven-257 {w['precision']} worst coefs={worst_c:.2e} values={worst_y:.2e}")
 
 
 def test_long_lines_fall_back_to_narrower_tiles():
@@ -123,3 +131,53 @@ def test_long_lines_fall_back_to_narrower_tiles():
     e(y, xs, c)
     torch.cuda.synchronize()
     assert float((y - vals).abs().max()) <= 1e-10
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_refine"])
+def test_config4_full_every_problem(oracle_mod, precision):
+    """The uneven workload at its named size -- 4096 problems, 3.47 M points, degrees 1-5, three
+    closures, uniform and perturbed meshes -- in one graph launch, every problem against the
+    oracle's FP64 build and evaluation: <= 1e-12 relative per problem (coefficients; values
+    relative to max(|values|, |coefficients|)), or 10 cond(A) eps for a problem whose matrix is
+    ill-conditioned enough to need it."""
+    import ddc_b200 as D
+    from ddc_b200 import workloads as W
+
+    O = oracle_mod
+    D.load_library()
+    probs = W.config4()
+    w = W.config4_batch(D, probs, precision=precision)
+    batch = D.UnevenBatch(w["builders"], w["evaluators"], w["nevals"])
+    cu = lambda a: torch.from_numpy(a).cuda()
+    info = batch.info
+    coefs = torch.full((info.total_coefs,), float("nan"), dtype=torch.float64, device="cuda")
+    out = torch.full((info.total_evals,), float("nan"), dtype=torch.float64, device="cuda")
+    batch(cu(w["vals"]), cu(w["dlo"]), cu(w["dhi"]), coefs, cu(w["coords"]), out)
+    coefs, out = coefs.cpu().numpy(), out.cpu().numpy()
+    off = batch.offsets()
+    clos = {"periodic": O.PERIODIC, "hermite": O.HERMITE, "greville": O.GREVILLE}
+    worst_c = worst_y = 0.0
+    for i, p in enumerate(probs):
+        b = w["builders"][i]
+        per = p["closure"] == "periodic"
+        obs = (O.BSplines(p["degree"], per, rmin=0.0, rmax=1.0, ncells=p["ncells"]) if p["uniform"]
+               else O.BSplines(p["degree"], per, breaks=p["breaks"]))
+        c = clos[p["closure"]]
+        ob = O.Builder(obs, b.interpolation_points, c, c)
+        herm = p["closure"] == "hermite"
+        lo = w["dlo"][off["derivs_lo"][i]:off["derivs_lo"][i + 1]]
+        hi = w["dhi"][off["derivs_hi"][i]:off["derivs_hi"][i + 1]]
+        ref = ob(w["vals"][off["vals"][i]:off["vals"][i + 1]], lo.reshape(-1, 1) if herm else None,
+                 hi.reshape(-1, 1) if herm else None)[:, 0]
+        x = w["coords"][off["evals"][i]:off["evals"][i + 1]]
+        ev = O.evaluate(obs, x[:, None], ref[:, None])[:, 0]
+        ec = np.abs(coefs[off["coefs"][i]:off["coefs"][i + 1]] - ref).max() / np.abs(ref).max()
+        # the B-splines sum to one, so a value's error is at most the largest coefficient error:
+        # values are compared relative to max(|values|, |coefficients|) (even-degree Hermite
+        # closures give boundary coefficients hundreds of times the values they produce)
+        ey = np.abs(out[off["evals"][i]:off["evals"][i + 1]] - ev).max() / max(np.abs(ev).max(), np.abs(ref).max())
+        if max(ec, ey) > 1e-12:
+            tol = 10 * np.linalg.cond(ob.matrix()) * np.finfo(float).eps
+            assert max(ec, ey) <= tol, (i, p["ncells"], p["degree"], p["closure"], ec, ey, tol)
+        worst_c, worst_y = max(worst_c, ec), max(worst_y, ey)
+    print(f"PARITY config4 {precision} 4096 problems worst coefs={worst_c:.2e} values={worst_y:.2e}")
