@@ -181,17 +181,19 @@ __global__ void __launch_bounds__(kEvalThreads, 4) uneven_eval_kernel(const __gr
     __syncthreads();
     if (live == 0) return;
     double* y = A.out + seg.x + threadIdx.x;
-    switch (se.degree * 2 + se.uniform) {
-    case 2: eval_seg<1, false>(se, A.coefs, xv, y, live); break;
-    case 3: eval_seg<1, true>(se, A.coefs, xv, y, live); break;
-    case 4: eval_seg<2, false>(se, A.coefs, xv, y, live); break;
-    case 5: eval_seg<2, true>(se, A.coefs, xv, y, live); break;
-    case 6: eval_seg<3, false>(se, A.coefs, xv, y, live); break;
-    case 7: eval_seg<3, true>(se, A.coefs, xv, y, live); break;
-    case 8: eval_seg<4, false>(se, A.coefs, xv, y, live); break;
-    case 9: eval_seg<4, true>(se, A.coefs, xv, y, live); break;
-    case 10: eval_seg<5, false>(se, A.coefs, xv, y, live); break;
-    default: eval_seg<5, true>(se, A.coefs, xv, y, live); break;
+    // a register copy, for the reason the build kernel keeps one of its tables
+    UnevenEval const e = se;
+    switch (e.degree * 2 + e.uniform) {
+    case 2: eval_seg<1, false>(e, A.coefs, xv, y, live); break;
+    case 3: eval_seg<1, true>(e, A.coefs, xv, y, live); break;
+    case 4: eval_seg<2, false>(e, A.coefs, xv, y, live); break;
+    case 5: eval_seg<2, true>(e, A.coefs, xv, y, live); break;
+    case 6: eval_seg<3, false>(e, A.coefs, xv, y, live); break;
+    case 7: eval_seg<3, true>(e, A.coefs, xv, y, live); break;
+    case 8: eval_seg<4, false>(e, A.coefs, xv, y, live); break;
+    case 9: eval_seg<4, true>(e, A.coefs, xv, y, live); break;
+    case 10: eval_seg<5, false>(e, A.coefs, xv, y, live); break;
+    default: eval_seg<5, true>(e, A.coefs, xv, y, live); break;
     }
 }
 
