@@ -17,7 +17,7 @@
 // gathers the right-hand side, runs the chunked tile solve of the batched builder (the chunks'
 // carries chained by the log-depth scan across the block's threads) and stores the coefficients.
 // Each group's evaluation kernel, which depends on that group's build kernel only, evaluates the
-// group's points from the stored coefficients with 256-thread blocks over segments of 512 points,
+// group's points from the stored coefficients with 256-thread blocks over segments of 1024 points,
 // so the points of a problem are spread over many threads instead of waiting on its chunk
 // threads, and the short problems' evaluations overlap the long problems' builds. The build
 // kernels of the groups with the longest problems get the highest stream priorities.
@@ -94,7 +94,7 @@ struct UnevenEvalArgs
 constexpr int kUnevenUnroll = 4;
 constexpr bool kUnevenScanPrefetch = false;
 constexpr int kEvalThreads = 256;
-constexpr int kEvalPts = 2;                           // points per thread
+constexpr int kEvalPts = 4;                           // points per thread
 constexpr int kSegment = kEvalThreads * kEvalPts;     // points per evaluation block
 
 namespace {
