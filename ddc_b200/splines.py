@@ -486,7 +486,8 @@ class SplineEvaluator2D:
 
 class UnevenBatch:
     """Many independent one-line problems (own builder and evaluator each) built and evaluated by
-    one graph launch of persistent kernels (ddcb_batch_uneven_*). Data are packed flat CUDA float64
+    one graph launch (ddcb_batch_uneven_*): per group of problems a build kernel with a block per
+    problem, then an evaluation kernel over the group's points. Data are packed flat CUDA float64
     arrays; `offsets()` gives every problem's slice. The builders and evaluators are kept alive by
     the batch."""
 

@@ -235,9 +235,12 @@ ddcb_status ddcb_build_eval_adjoint(ddcb_builder b, ddcb_evaluator e, int32_t or
                                     ddcb_lines g_coords_layout, int32_t* fused, ddcb_stream stream);
 
 /* ---- uneven batch: many independent one-line problems (each its own builder and evaluator:
- *      size, degree, closure and mesh may all differ) built and evaluated by persistent kernels
- *      in one CUDA graph launch (no reference counterpart: the reference loops one SplineBuilder
- *      per problem). The builders and evaluators must outlive the batch; each solves in its own
+ *      size, degree, closure and mesh may all differ) built and evaluated in one CUDA graph
+ *      launch: per group of problems (band shape, arithmetic, block size) a build kernel with a
+ *      block per problem, then an evaluation kernel over the group's points (no reference
+ *      counterpart: the reference loops one SplineBuilder per problem). A builder solves fastest
+ *      here when its chunk count fills whole warps (32 chunks per warp). The builders and
+ *      evaluators must outlive the batch; each solves in its own
  *      precision (FP64, or FP32 with refinement, whose convergence ddcb_builder_device_status
  *      reports per builder). Data are packed: problem i's samples at
  *      vals[vals_off[i] .. vals_off[i+1]), its Hermite derivatives likewise in derivs_lo /
