@@ -74,6 +74,17 @@ void dispatch(BuildArgs const& args, int TL, cudaStream_t s)
     else throw Error(DDCB_ERR_UNSUPPORTED, "band shape kl=" + std::to_string(kl) + " ku=" + std::to_string(ku) + " has no kernel");
 }
 
+// Point threads per line of the fused kernels (tiles of 8 lines): 64 (512-thread blocks, two per
+// SM), or 128 (1024 threads, one per SM) when the batch gives fewer tiles than SMs and each SM
+// evaluates a whole tile alone (1000 lines: 28.9 -> 26.9 us).
+int fused_point_threads(int64_t nlines)
+{
+    int dev = 0, sms = 0;
+    DDCB_CUDA_CHECK(cudaGetDevice(&dev));
+    DDCB_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    return (nlines + 7) / 8 < sms ? 128 : 64;
+}
+
 int pick_nct(SolveTables const& t, int TL)
 {
     // threads per line pair: one per chunk, rounded so the block is whole warps (at least two);
@@ -127,8 +138,8 @@ bool launch_build_eval(Builder const& b, Evaluator const& e, int order, double* 
     bool fused = false;
     if (b.tile_lines == 8 && b.precision == DDCB_FP64) {
         BuildArgs args = make_build_args(b, coefs, lc, vals, lv, dlo, llo, dhi, lhi);
-        // the evaluation part uses every thread: 64 point threads per line (512 per block)
-        args.nct = std::max(args.nct, 64);
+        // the evaluation part uses every thread
+        args.nct = std::max(args.nct, fused_point_threads(args.nlines));
         fused = launch_build_eval_fused(args, e, order, out, lo, coords, lx, s);
     }
     if (!fused) {
@@ -158,7 +169,7 @@ bool launch_advect(Builder const& b, Evaluator const& e, double dt, double const
     if (nl == 0 || m == 0) return true;
     if (b.tile_lines == 8 && b.precision == DDCB_FP64) {
         BuildArgs args = make_build_args(b, coefs, lc, vals, lv, dlo, llo, dhi, lhi);
-        args.nct = std::max(args.nct, 64);
+        args.nct = std::max(args.nct, fused_point_threads(args.nlines));
         if (launch_advect_fused(args, e, b.d_points, dt, velocity, v_const, v_div, out, lo, s)) return true;
     }
     // build, feet, evaluate: the coefficients and the feet in stream-ordered scratch
