@@ -9,7 +9,9 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libddcb.so")
+# DDCB_CHECK_BOUNDS=1 in the environment selects the bounds-checked build (libddcb_check.so): the
+# same kernels, each computed array index checked on the device (ddcb_last_device_error)
+LIB_PATH = os.path.join(HERE, "libddcb_check.so" if os.environ.get("DDCB_CHECK_BOUNDS") == "1" else "libddcb.so")
 
 # enums (include/ddcb.h)
 PERIODIC, HERMITE, HOMOGENEOUS_HERMITE, GREVILLE = 0, 1, 2, 3
@@ -83,6 +85,7 @@ SIGNATURES = {
     "ddcb_builder_destroy": [_vp],
     "ddcb_builder_get_info": [_vp, C.POINTER(BuilderInfo)],
     "ddcb_builder_device_status": [_vp, _vp],
+    "ddcb_last_device_error": [_vp],
     "ddcb_build": [_vp, _vp, Lines, _vp, Lines, _vp, Lines, _vp, Lines, _vp],
     "ddcb_solve_multirhs": [_vp, _vp, C.c_int64, C.c_int64, C.c_int32, _vp],
     "ddcb_quadrature_coefficients": [_vp, _vp, _vp, _vp],
@@ -139,6 +142,8 @@ def load():
     L.ddcb_status_string.restype = C.c_char_p
     L.ddcb_last_error_message.argtypes = []
     L.ddcb_last_error_message.restype = C.c_char_p
+    L.ddcb_bounds_checked.argtypes = []
+    L.ddcb_bounds_checked.restype = C.c_int32
     _lib = L
     return L
 

@@ -1,6 +1,8 @@
-"""Build the CUDA library libddcb.so in-tree for sm_100a (B200).
+"""Build the CUDA library libddcb.so in-tree for sm_100a (B200), and its bounds-checked variant
+libddcb_check.so (the same sources with -DDDCB_CHECK_BOUNDS: every computed array index checked
+on the device, reported by ddcb_last_device_error).
 
-    python -m ddc_b200.build        (or ddc_b200.build.build())
+    python -m ddc_b200.build [--check-bounds]        (or ddc_b200.build.build())
 """
 from __future__ import annotations
 
@@ -11,6 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libddcb.so")
+LIB_CHECK = os.path.join(HERE, "libddcb_check.so")
 SOURCES = ["api.cu", "plan.cpp", "build_kernels.cu", "eval_kernels.cu", "fused_kernels.cu", "tensor2d.cu",
            "adjoint_kernels.cu", "refine_kernels.cu",
            "uneven_batch.cu", "host_pipeline.cu", "quadrature.cu", "tensornd.cu"]
@@ -28,24 +31,28 @@ def sources():
     return [os.path.join(CSRC, s) for s in SOURCES]
 
 
-def needs_build() -> bool:
-    if not os.path.exists(LIB):
+def needs_build(lib: str = LIB) -> bool:
+    if not os.path.exists(lib):
         return True
-    t = os.path.getmtime(LIB)
+    t = os.path.getmtime(lib)
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "ddcb.h")]
     return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
 
 
-def build(verbose: bool = False, force: bool = False) -> str:
-    """Compile every source to an object in parallel, then link libddcb.so."""
-    if not force and not needs_build():
-        return LIB
+def build(verbose: bool = False, force: bool = False, check_bounds: bool = False) -> str:
+    """Compile every source to an object in parallel, then link libddcb.so (libddcb_check.so with
+    check_bounds)."""
+    lib = LIB_CHECK if check_bounds else LIB
+    if not force and not needs_build(lib):
+        return lib
     from concurrent.futures import ThreadPoolExecutor
 
-    objdir = os.path.join(HERE, "_build")
+    objdir = os.path.join(HERE, "_build_check" if check_bounds else "_build")
     os.makedirs(objdir, exist_ok=True)
     common = [nvcc(), "-std=c++17", "-O3", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-ccbin", "g++",
               "--expt-relaxed-constexpr"]
+    if check_bounds:
+        common.append("-DDDCB_CHECK_BOUNDS")
     if verbose:
         common.append("-Xptxas=-v")
 
@@ -72,11 +79,10 @@ def build(verbose: bool = False, force: bool = False) -> str:
             sys.stderr.write(r.stderr)
         if r.returncode:
             raise subprocess.CalledProcessError(r.returncode, src)
-    link = [nvcc(), *ARCH, "-shared", "-o", LIB, *[o for _, o, _ in results]]
+    link = [nvcc(), *ARCH, "-shared", "-o", lib, *[o for _, o, _ in results]]
     subprocess.run(link, check=True)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
-    build(verbose="-v" in sys.argv, force=True)
-    print(LIB)
+    print(build(verbose="-v" in sys.argv, force=True, check_bounds="--check-bounds" in sys.argv))

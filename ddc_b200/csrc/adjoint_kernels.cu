@@ -328,7 +328,7 @@ __device__ __forceinline__ void scatter_points(EvalAdjointArgs const& a, EvalBas
             double w[D + 1], unused;
             int const jmin = point_adjoint<D, ORDER, UNI>(eb, a.ex_lo, a.ex_hi, xs[u], none, false, w, unused);
             if (jmin >= 0) {
-                int const r0 = rows.row0(jmin);
+                int const r0 = rows.row0(DDCB_INDEX(jmin, eb.b.ncells));
 #pragma unroll
                 for (int i = 0; i < D + 1; ++i) atomicAdd(G + rows.row(r0, i) * TLE + l, gs[u] * w[i]);
             }

@@ -10,6 +10,7 @@
 
 #include <nvtx3/nvToolsExt.h>
 
+#include "check_bounds.cuh"
 #include "ddcb_internal.hpp"
 
 struct ddcb_bsplines_t
@@ -170,9 +171,60 @@ void destroy_evaluator(Evaluator* e)
     delete e;
 }
 
+// The readers of the translation units' bounds-event words (bounds-checked build only; a
+// function-local static, so the units' load-time registrations find it constructed).
+std::vector<BoundsReader>& bounds_readers()
+{
+    static std::vector<BoundsReader> readers;
+    return readers;
+}
+
+void register_bounds_reader(BoundsReader r) { bounds_readers().push_back(r); }
+
+// The file of a recorded event, from its tag (the device sources and headers that name indices).
+std::string bounds_site_name(unsigned long long site)
+{
+    static char const* const files[] = {"build_device.cuh", "eval_device.cuh", "refine_device.cuh", "adjoint_kernels.cu",
+                                        "build_kernels.cu", "eval_kernels.cu", "fused_kernels.cu", "tensor2d.cu",
+                                        "tensornd.cu", "uneven_batch.cu", "quadrature.cu", "refine_kernels.cu",
+                                        "host_pipeline.cu", "api.cu"};
+    uint32_t const tag = uint32_t(site >> 16) & 0xFFFFu;
+    std::string name = "unknown file";
+    for (char const* f : files)
+        if (bounds_file_tag(f) == tag) name = f;
+    return name + ":" + std::to_string(site & 0xFFFFull);
+}
+
 } // namespace ddcb
 
 extern "C" {
+
+int32_t ddcb_bounds_checked(void)
+{
+#ifdef DDCB_CHECK_BOUNDS
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+ddcb_status ddcb_last_device_error(ddcb_stream stream)
+{
+    return guarded(__func__, [&] {
+        cudaError_t const e = cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream));
+        if (e != cudaSuccess)
+            throw ddcb::Error(DDCB_ERR_CUDA, std::string("a kernel queued on this stream failed: ") + cudaGetErrorString(e));
+        // every unit's event is read (and so cleared); the first one found is reported
+        std::string first;
+        for (ddcb::BoundsReader r : ddcb::bounds_readers()) {
+            ddcb::BoundsEvent ev {};
+            if (r(&ev) && first.empty())
+                first = "index " + std::to_string(ev.index) + " outside [0, " + std::to_string(ev.bound) + ") at "
+                        + ddcb::bounds_site_name(ev.site) + " (the kernel went on with the index clamped)";
+        }
+        if (!first.empty()) throw ddcb::Error(DDCB_ERR_DEVICE, first);
+    });
+}
 
 const char* ddcb_status_string(ddcb_status s)
 {

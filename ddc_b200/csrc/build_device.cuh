@@ -18,6 +18,7 @@
 
 #include <type_traits>
 
+#include "check_bounds.cuh"
 #include "ddcb_internal.hpp"
 
 namespace ddcb {
@@ -386,7 +387,7 @@ __device__ __forceinline__ double rhs_row(BuildArgs const& args, int r, int64_t 
     int const v1 = (args.raw || R.periodic) ? n : R.nbe_lo + R.npoints;
     int sr = r + R.lrot;
     sr -= (sr >= n) ? n : 0;
-    if (sr >= v0 && sr < v1) return args.vals[(int64_t)(sr - v0) * args.lv.stride + line_offset(args.lv, line)];
+    if (sr >= v0 && sr < v1) return args.vals[(int64_t)DDCB_INDEX(sr - v0, v1 - v0) * args.lv.stride + line_offset(args.lv, line)];
     if (sr < R.nbe_lo) return sr < R.nbv_lo ? args.dlo[sr * args.llo.stride + line_offset(args.llo, line)] * R.dxpow_lo[sr] : 0.0;
     int const i = sr - (n - R.nbe_hi);
     return i < R.nbv_hi ? args.dhi[i * args.lhi.stride + line_offset(args.lhi, line)] * R.dxpow_hi[i] : 0.0;
@@ -428,7 +429,7 @@ __device__ __forceinline__ void gather_tile(BuildArgs const& args, double* T)
             double* dst = T + r * TL + 2 * p;
             if (sr >= v0 && sr < v1) {
                 if (live1) {
-                    cp_async16(dst, args.vals + (int64_t)(sr - v0) * args.lv.stride + ov);
+                    cp_async16(dst, args.vals + (int64_t)DDCB_INDEX(sr - v0, v1 - v0) * args.lv.stride + ov);
                 } else {
                     dst[0] = live0 ? args.vals[(int64_t)(sr - v0) * args.lv.stride + ov] : 0.0;
                     dst[1] = 0.0;
@@ -447,7 +448,7 @@ __device__ __forceinline__ void gather_tile(BuildArgs const& args, double* T)
         for (int r = c; r < n; r += nct) {
             int sr = r + R.lrot;
             sr -= (sr >= n) ? n : 0;
-            if (live && sr >= v0 && sr < v1) cp_async8(T + r * TL + l, args.vals + (int64_t)(sr - v0) * args.lv.stride + ov);
+            if (live && sr >= v0 && sr < v1) cp_async8(T + r * TL + l, args.vals + (int64_t)DDCB_INDEX(sr - v0, v1 - v0) * args.lv.stride + ov);
             else T[r * TL + l] = live && !(sr >= v0 && sr < v1) ? other_row(sr, line) : 0.0;
         }
     }
@@ -492,7 +493,7 @@ __device__ __forceinline__ void store_tile(BuildArgs const& args, const double* 
         int64_t const oo = line_offset(args.lo, line);
         bool const live1 = line + 1 < args.nlines;
         for (int r = c2; r < rows; r += 2 * args.nct) {
-            double2 const v = *reinterpret_cast<const double2*>(T + coef_row(args.r, n, r) * TL + 2 * p);
+            double2 const v = *reinterpret_cast<const double2*>(T + DDCB_INDEX(coef_row(args.r, n, r), n) * TL + 2 * p);
             double* dst = args.out + r * args.lo.stride + oo;
             if (live1) __stcs(reinterpret_cast<double2*>(dst), v);
             else __stcs(dst, v.x);
@@ -504,7 +505,7 @@ __device__ __forceinline__ void store_tile(BuildArgs const& args, const double* 
     int64_t const line = tile_line0<TL>(args) + l;
     if (line >= args.nlines) return;
     int64_t const oo = line_offset(args.lo, line);
-    for (int r = c; r < rows; r += args.nct) __stcs(args.out + r * args.lo.stride + oo, T[coef_row(args.r, n, r) * TL + l]);
+    for (int r = c; r < rows; r += args.nct) __stcs(args.out + r * args.lo.stride + oo, T[DDCB_INDEX(coef_row(args.r, n, r), n) * TL + l]);
 }
 
 } // namespace ddcb

@@ -8,6 +8,7 @@
 #pragma once
 
 #include "bspline_math.cuh"
+#include "check_bounds.cuh"
 
 namespace ddcb {
 
@@ -113,7 +114,7 @@ __device__ __forceinline__ int nonuniform_walk(EvalBasis const& eb, double x, in
 __device__ __forceinline__ int nonuniform_locate(EvalBasis const& eb, double x)
 {
     int const c = nonuniform_guess(eb, x);
-    double2 const p = eb.kpairs[c];
+    double2 const p = eb.kpairs[DDCB_INDEX(c, eb.nk - 1)];
     return nonuniform_is_cell(eb, x, c, p.x, p.y) ? c : nonuniform_walk(eb, x, c);
 }
 
@@ -123,7 +124,7 @@ __device__ __forceinline__ void load_knots(EvalBasis const& eb, int c, double* k
 {
 #pragma unroll
     for (int q = 0; q < P; ++q) {
-        double2 const p = eb.kpairs[c - P + 1 + 2 * q];
+        double2 const p = eb.kpairs[DDCB_INDEX(c - P + 1 + 2 * q, eb.nk - 1)];
         kn[2 * q] = p.x;
         kn[2 * q + 1] = p.y;
     }
@@ -277,7 +278,7 @@ __device__ __forceinline__ double nonuniform_deriv1(EvalBasis const& eb, double 
         inv *= d[i - 1];
     }
     f[1] = inv;
-    int const r0 = C.row0(ck - D);
+    int const r0 = C.row0(DDCB_INDEX(ck - D, eb.b.ncells));
     double y = 0.0;
     double cprev = C.get(r0, 0);
 #pragma unroll
@@ -302,7 +303,7 @@ __device__ __forceinline__ double nonuniform_deriv1_dcoef(EvalBasis const& eb, d
     int const ck = locate_load_knots<P>(eb, x, kn);
     double v[P + 1];
     nonuniform_values_div<P>(kn, x, v);
-    int const r0 = C.row0(ck - P);
+    int const r0 = C.row0(DDCB_INDEX(ck - D, eb.b.ncells) + 1);
     double y = 0.0;
 #pragma unroll
     for (int r = 0; r < P + 1; ++r) y = fma(C.get(r0, r), v[r], y);
@@ -324,7 +325,7 @@ __device__ __forceinline__ double eval_value_no_bc(EvalBasis const& eb, double x
         jmin = locate_load_knots<D>(eb, x, kn) - D;
         nonuniform_values_div<D>(kn, x, v);
     }
-    int const r0 = C.row0(jmin);
+    int const r0 = C.row0(DDCB_INDEX(jmin, eb.b.ncells));
     double y = 0.0;
 #pragma unroll
     for (int i = 0; i < D + 1; ++i) y = fma(C.get(r0, i), v[i], y);
@@ -380,7 +381,7 @@ __device__ __forceinline__ double eval_deriv_no_bc(EvalBasis const& eb, double x
         }
     }
     const double* dspan = eb.inv_span + jmin; // 1/(t[jmin+i+len] - t[jmin+i]) at dspan[(len-1)*nk + i]
-    int const r0 = C.row0(jmin);
+    int const r0 = C.row0(DDCB_INDEX(jmin, eb.b.ncells));
 #pragma unroll
     for (int i = 0; i < D + 1; ++i) cc[i] = C.get(r0, i);
 #pragma unroll
@@ -509,7 +510,7 @@ __device__ __forceinline__ int point_adjoint(EvalBasis const& eb, int ex_lo, int
         }
         if (want_dx && !fixed) {
             // s'(x) = sum_r cc[r+1] B_{jmin+1+r, D-1}(x), cc the first divided differences
-            int const r0 = C.row0(jmin);
+            int const r0 = C.row0(DDCB_INDEX(jmin, eb.b.ncells));
             double cprev = C.get(r0, 0);
             double y = 0.0;
 #pragma unroll

@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(32 * kPtsNd) evalnd_kernel(const __grid_consta
         if (!done) {
             double v[kMaxDims][kMaxDegree + 1];
             int jmin[kMaxDims];
-            for (int d = 0; d < N; ++d) jmin[d] = basis_rt(a.eb[d], a.deriv ? a.order[d] : 0, x[d], v[d]);
+            for (int d = 0; d < N; ++d) jmin[d] = DDCB_INDEX(basis_rt(a.eb[d], a.deriv ? a.order[d] : 0, x[d], v[d]), a.eb[d].b.ncells);
             y = tensor_sum(a, C, jmin, v);
         }
         a.out[p * a.B + b] = y;
@@ -283,9 +283,9 @@ __global__ void __launch_bounds__(32 * kPtsNd) eval3d_kernel(const __grid_consta
         }
         if (!zero) {
             double v0[D + 1], v1[D + 1], v2[D + 1];
-            int const j0 = basis_values_any<D>(a.eb[0], x[0], v0);
-            int const j1 = basis_values_any<D>(a.eb[1], x[1], v1);
-            int const j2 = basis_values_any<D>(a.eb[2], x[2], v2);
+            int const j0 = DDCB_INDEX(basis_values_any<D>(a.eb[0], x[0], v0), a.eb[0].b.ncells);
+            int const j1 = DDCB_INDEX(basis_values_any<D>(a.eb[1], x[1], v1), a.eb[1].b.ncells);
+            int const j2 = DDCB_INDEX(basis_values_any<D>(a.eb[2], x[2], v2), a.eb[2].b.ncells);
 #pragma unroll
             for (int i0 = 0; i0 <= D; ++i0) {
                 double t1 = 0.0;

@@ -101,6 +101,17 @@ typedef struct ddcb_builder_info {
 /* ---- status ---------------------------------------------------------------------------- */
 const char* ddcb_status_string(ddcb_status s);
 const char* ddcb_last_error_message(void);
+/* Device-side failures of the work queued on `stream` so far (SURVEY's ddcb_last_device_error;
+ * the reference's debug builds assert the same index ranges with KOKKOS_ASSERT,
+ * bsplines_uniform.hpp:489-494, bsplines_non_uniform.hpp:469-479): waits for the stream; returns
+ * DDCB_ERR_CUDA if a kernel failed, and, in the bounds-checked build (libddcb_check.so, built with
+ * -DDDCB_CHECK_BOUNDS), DDCB_ERR_DEVICE for the first computed index (cell, knot pair, tile row)
+ * that a kernel found outside its array since the previous call -- file, line, index and bound in
+ * ddcb_last_error_message(); the kernel went on with the index clamped into range. Refinement
+ * convergence is reported per builder by ddcb_builder_device_status. */
+ddcb_status ddcb_last_device_error(ddcb_stream stream);
+/* 1 in the bounds-checked build, 0 in the default one. */
+int32_t ddcb_bounds_checked(void);
 
 /* ---- basis: UniformBSplines<CDim,D>::Impl(rmin, rmax, ncells) (bsplines_uniform.hpp:145-155)
  *      and NonUniformBSplines<CDim,D>::Impl(breaks) (bsplines_non_uniform.hpp:414-457). ------- */

@@ -27,6 +27,40 @@ def test_library_exports_every_declared_symbol():
         assert hasattr(L, n), n
 
 
+def test_bounds_checked_build_exports_the_same_symbols():
+    """libddcb_check.so (the DDCB_CHECK_BOUNDS build) exports every declared symbol and says it is
+    the checked build; the default library says it is not."""
+    import ddc_b200
+
+    path = os.path.join(ROOT, "ddc_b200", "libddcb_check.so")
+    if not os.path.exists(path):
+        pytest.skip("libddcb_check.so not built")
+    L = C.CDLL(path)
+    for n in declared_functions():
+        assert hasattr(L, n), n
+    L.ddcb_bounds_checked.restype = C.c_int32
+    assert L.ddcb_bounds_checked() == 1
+    assert ddc_b200.bounds_checked() is False
+
+
+def test_bounds_site_tags_are_distinct(tmp_path):
+    """The file tags that name the site of a recorded out-of-range index are distinct for every
+    device source and header (check_bounds.cuh's 16-bit hash of the base name)."""
+    import shutil
+    import subprocess
+
+    if shutil.which("g++") is None:
+        pytest.skip("needs g++")
+    files = sorted(f for f in os.listdir(os.path.join(ROOT, "ddc_b200", "csrc")) if f.endswith((".cu", ".cuh")))
+    src = tmp_path / "tags.cpp"
+    src.write_text('#include <cstdio>\n#include "check_bounds.cuh"\nint main(){\n'
+                   + "".join(f'std::printf("%u\\n", ddcb::bounds_file_tag("dir/{f}"));\n' for f in files) + "}\n")
+    exe = str(tmp_path / "tags")
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "ddc_b200", "csrc"), str(src), "-o", exe], check=True)
+    tags = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
+    assert len(tags) == len(files) and len(set(tags)) == len(tags)
+
+
 def test_status_strings():
     import ddc_b200
 
