@@ -921,6 +921,12 @@ static void check_valid_grid(Builder const& b)
     if (long(b.points.size()) != expected)
         throw Error(DDCB_ERR_BAD_GRID, "Incorrect number of points supplied to NonUniformInterpolationPoints. (Received : "
                                            + std::to_string(b.points.size()) + ", expected : " + std::to_string(expected));
+    // A periodic basis of ncells <= degree wraps each B-spline onto itself (its support is longer
+    // than the period), and the offset rule (spline_builder.hpp:619-658) reads interpolation point
+    // number `degree`, which such a grid does not have.
+    if (D.periodic && D.ncells <= D.degree)
+        throw Error(DDCB_ERR_BAD_GRID, "a periodic basis of degree " + std::to_string(D.degree) + " needs more than "
+                                           + std::to_string(D.degree) + " cells (got " + std::to_string(D.ncells) + ")");
     int in_cell = 0;
     long cell_end = D.degree + 1;
     auto check = [&](int npc, long cend) {
