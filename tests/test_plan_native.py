@@ -40,3 +40,22 @@ def test_plan_matrix_equals_reference_matrix(tmp_path, oracle_mod):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-3000:]
     assert "0 failures" in r.stdout
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_plan_under_sanitizers(tmp_path):
+    """The plan code compiled with AddressSanitizer and UndefinedBehaviorSanitizer: the device-solve
+    emulation of every plan_check case, and a sweep of tiny grids (1-15 cells, every degree, closure
+    and mesh kind) that must plan or be refused without touching memory outside its arrays."""
+    cuda_inc = "/usr/local/cuda/include"
+    flags = ["-std=c++17", "-O1", "-g", "-fsanitize=address,undefined", "-fno-sanitize-recover=undefined",
+             f"-I{cuda_inc}"]
+    for name in ("plan_check", "small_grids_check"):
+        exe = str(tmp_path / name)
+        cmd = ["g++", *flags, "-x", "c++", os.path.join(ROOT, "ddc_b200", "csrc", "plan.cpp"),
+               os.path.join(ROOT, "tests", "native", name + ".cpp"), "-x", "none", "-L/usr/local/cuda/lib64", "-lcudart",
+               "-o", exe]
+        subprocess.run(cmd, check=True, capture_output=True)
+        env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0")
+        r = subprocess.run([exe], capture_output=True, text=True, timeout=900, env=env)
+        assert r.returncode == 0, (name, r.stdout[-2000:], r.stderr[-3000:])
