@@ -121,7 +121,9 @@ __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const __grid_constan
     int64_t const oo = line_offset(a.lo, line);
     int64_t const m = a.lx.n;
     CoefDirect const acc {C + l, TLE};
-    constexpr int U = 8; // points in flight per thread
+    // points in flight per thread: 16 for the derivative spline (its coordinates loaded together,
+    // 0.78 -> 0.73 ms on 65536 quintic lines), 8 elsewhere (16 spills the other variants)
+    constexpr int U = DSPLINE ? 16 : 8;
     int64_t const sx = a.lx.stride * nct, so = a.lo.stride * nct;
     const double* __restrict__ xp = a.coords + ox + c * a.lx.stride;
     double* __restrict__ op = a.out + oo + c * a.lo.stride;
