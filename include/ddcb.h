@@ -101,8 +101,8 @@ typedef struct ddcb_builder_info {
 /* ---- status ---------------------------------------------------------------------------- */
 const char* ddcb_status_string(ddcb_status s);
 const char* ddcb_last_error_message(void);
-/* Device-side failures of the work queued on `stream` so far (SURVEY's ddcb_last_device_error;
- * the reference's debug builds assert the same index ranges with KOKKOS_ASSERT,
+/* Device-side failures of the work queued on `stream` so far (the reference's debug builds
+ * assert the same index ranges with KOKKOS_ASSERT,
  * bsplines_uniform.hpp:489-494, bsplines_non_uniform.hpp:469-479): waits for the stream; returns
  * DDCB_ERR_CUDA if a kernel failed, and, in the bounds-checked build (libddcb_check.so, built with
  * -DDDCB_CHECK_BOUNDS), DDCB_ERR_DEVICE for the first computed index (cell, knot pair, tile row)
