@@ -53,7 +53,11 @@ void launch_build2d(Builder const& b1, Builder const& b2, double* coefs, double 
     int64_t const s1 = b1.basis.size(), s2 = b2.basis.size();
     int64_t const nlo1 = b1.nbv_lo, nhi1 = b1.nbv_hi, nlo2 = b2.nbv_lo, nhi2 = b2.nbv_hi;
     bool const her_lo2 = b2.lo == DDCB_HERMITE && nlo2 > 0, her_hi2 = b2.hi == DDCB_HERMITE && nhi2 > 0;
-    int64_t const G0 = group_fields(b1, b2, B, max_group);
+    // groups of equal size (64 fields in groups of at most 19: 16, 16, 16, 16 rather than 19, 19, 19, 7,
+    // whose last group would fill a third of the GPU); the workspace holds the cap's group
+    int64_t const Gcap = group_fields(b1, b2, B, max_group);
+    int64_t const ngroups = (B + Gcap - 1) / std::max<int64_t>(Gcap, 1);
+    int64_t const G0 = ngroups > 0 ? (B + ngroups - 1) / ngroups : Gcap;
     Lines const none {0, 1, 0, 0, 0};
     double* S1 = ws;                        // (s1, np2, G0): one group's x1 pass over the values
     double* S1lo = S1 + s1 * np2 * G0;      // (s1, nlo2, B): every field's lower derivative slab
