@@ -1048,7 +1048,7 @@ ddcb_status ddcb_build2d(ddcb_builder h1, ddcb_builder h2, double* coefs, const 
             ddcb::launch_build2d(b1, b2, coefs, vals, h1lo ? dmin1 : nullptr, h1hi ? dmax1 : nullptr, h2lo ? dmin2 : nullptr,
                                  h2hi ? dmax2 : nullptr, (h1lo && h2lo) ? m11 : nullptr, (h1hi && h2lo) ? m21 : nullptr,
                                  (h1lo && h2hi) ? m12 : nullptr, (h1hi && h2hi) ? m22 : nullptr, nbatch,
-                                 static_cast<double*>(ws), s);
+                                 static_cast<double*>(ws), s, 0, true);
         } catch (...) {
             if (owned) cudaFreeAsync(ws, s);
             throw;

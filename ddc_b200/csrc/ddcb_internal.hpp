@@ -301,7 +301,8 @@ void tune_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, do
 size_t build2d_workspace_bytes(Builder const& b1, Builder const& b2, int64_t nbatch);
 void launch_build2d(Builder const& b1, Builder const& b2, double* coefs, double const* vals, double const* dmin1,
                     double const* dmax1, double const* dmin2, double const* dmax2, double const* m11, double const* m21,
-                    double const* m12, double const* m22, int64_t B, double* ws, cudaStream_t s, int64_t max_group = 0);
+                    double const* m12, double const* m22, int64_t B, double* ws, cudaStream_t s, int64_t max_group = 0,
+                    bool overlap_slabs = false);
 void launch_eval2d(Evaluator const& e1, Evaluator const& e2, int o1, int o2, double* out, double const* coords,
                    double const* coefs, int64_t m, int64_t B, cudaStream_t s);
 void launch_integrate2d(Evaluator const& e1, Evaluator const& e2, double* out, double const* coefs, int64_t B, cudaStream_t s);

@@ -20,6 +20,33 @@ namespace ddcb {
 
 namespace {
 
+// A second stream of the calling host thread on the current device, with the two events of a
+// fork and a join: the 2D build runs its dim-2 derivative slab passes there, beside the first
+// group's value pass. Kept per host thread (calls of one thread are ordered), created on first use
+// and kept until the thread ends.
+struct SideStream
+{
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+
+SideStream& side_stream_for_current_device()
+{
+    thread_local SideStream side[16];
+    int dev = 0;
+    DDCB_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 16) throw Error(DDCB_ERR_UNSUPPORTED, "device ordinal above 15");
+    SideStream& ss = side[dev];
+    if (ss.stream == nullptr) {
+        DDCB_CUDA_CHECK(cudaStreamCreateWithFlags(&ss.stream, cudaStreamNonBlocking));
+        DDCB_CUDA_CHECK(cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming));
+        DDCB_CUDA_CHECK(cudaEventCreateWithFlags(&ss.join, cudaEventDisableTiming));
+        ss.device = dev;
+    }
+    return ss;
+}
+
 // Fields per group: the x1-pass result of a group stays near 40 MiB (L2-sized), and at most
 // max_group fields (0: no cap).
 int64_t group_fields(Builder const& b1, Builder const& b2, int64_t nbatch, int64_t max_group = 0)
@@ -47,7 +74,8 @@ size_t build2d_workspace_bytes(Builder const& b1, Builder const& b2, int64_t nba
 
 void launch_build2d(Builder const& b1, Builder const& b2, double* coefs, double const* vals, double const* dmin1,
                     double const* dmax1, double const* dmin2, double const* dmax2, double const* m11, double const* m21,
-                    double const* m12, double const* m22, int64_t B, double* ws, cudaStream_t s, int64_t max_group)
+                    double const* m12, double const* m22, int64_t B, double* ws, cudaStream_t s, int64_t max_group,
+                    bool overlap_slabs)
 {
     int64_t const np1 = int64_t(b1.points.size()), np2 = int64_t(b2.points.size());
     int64_t const s1 = b1.basis.size(), s2 = b2.basis.size();
@@ -65,21 +93,35 @@ void launch_build2d(Builder const& b1, Builder const& b2, double* coefs, double 
     // lines of an x1 pass over an (x1, q, ld) array, for G fields: (q, field)
     auto x1_lines = [&](int64_t n, int64_t nq, int64_t ld, int64_t G) { return Lines {n, nq * ld, G, nq, ld}; };
     // (a), (c) x1 passes over the dim-2 derivative slabs of all fields at once (a few rows per field:
-    // one launch each instead of one per group), with the mixed derivatives as Hermite data
+    // one launch each instead of one per group), with the mixed derivatives as Hermite data. They
+    // are short launches (a few blocks) whose latency a second stream hides behind the first group's
+    // value pass when overlap_slabs is set; the x2 passes wait for them.
+    SideStream* side = (overlap_slabs && (her_lo2 || her_hi2)) ? &side_stream_for_current_device() : nullptr;
+    cudaStream_t const ss = side ? side->stream : s;
+    if (side) {
+        DDCB_CUDA_CHECK(cudaEventRecord(side->fork, s));
+        DDCB_CUDA_CHECK(cudaStreamWaitEvent(ss, side->fork, 0));
+    }
     if (her_lo2) {
         launch_build(b1, S1lo, x1_lines(s1, nlo2, B, B), dmin2, x1_lines(np1, nlo2, B, B), m11,
-                     m11 ? x1_lines(nlo1, nlo2, B, B) : none, m21, m21 ? x1_lines(nhi1, nlo2, B, B) : none, s);
+                     m11 ? x1_lines(nlo1, nlo2, B, B) : none, m21, m21 ? x1_lines(nhi1, nlo2, B, B) : none, ss);
     }
     if (her_hi2) {
         launch_build(b1, S1hi, x1_lines(s1, nhi2, B, B), dmax2, x1_lines(np1, nhi2, B, B), m12,
-                     m12 ? x1_lines(nlo1, nhi2, B, B) : none, m22, m22 ? x1_lines(nhi1, nhi2, B, B) : none, s);
+                     m12 ? x1_lines(nlo1, nhi2, B, B) : none, m22, m22 ? x1_lines(nhi1, nhi2, B, B) : none, ss);
     }
+    if (side) DDCB_CUDA_CHECK(cudaEventRecord(side->join, ss));
+    bool joined = side == nullptr;
     for (int64_t f0 = 0; f0 < B; f0 += G0) {
         int64_t const G = std::min(G0, B - f0);
         // (b) x1 pass over the values of the group
         launch_build(b1, S1, x1_lines(s1, np2, G, G), vals + f0, x1_lines(np1, np2, B, G), dmin1 ? dmin1 + f0 : nullptr,
                      dmin1 ? x1_lines(nlo1, np2, B, G) : none, dmax1 ? dmax1 + f0 : nullptr,
                      dmax1 ? x1_lines(nhi1, np2, B, G) : none, s);
+        if (!joined) {
+            DDCB_CUDA_CHECK(cudaStreamWaitEvent(s, side->join, 0));
+            joined = true;
+        }
         // (d) x2 pass: lines (row r of the x1 coefficients, field) of the x1 results
         Lines const lv2 {np2, G, G, s1, np2 * G};
         Lines const llo2 {nlo2, B, G, s1, nlo2 * B};
@@ -88,6 +130,7 @@ void launch_build2d(Builder const& b1, Builder const& b2, double* coefs, double 
         launch_build(b2, coefs + f0, lc2, S1, lv2, her_lo2 ? S1lo + f0 : nullptr, her_lo2 ? llo2 : none,
                      her_hi2 ? S1hi + f0 : nullptr, her_hi2 ? lhi2 : none, s);
     }
+    if (!joined) DDCB_CUDA_CHECK(cudaStreamWaitEvent(s, side->join, 0));
 }
 
 namespace {

@@ -110,6 +110,22 @@ def test_build2d_explicit_workspace(oracle_mod):
     ws = torch.empty(b2d.workspace_bytes(B) // 8 + 1, dtype=torch.float64, device="cuda")
     b2d(c2, vals, None, None, dmin2, dmax2, workspace=ws)
     assert torch.equal(c1, c2)
+    # captured in a CUDA graph (the derivative-slab passes fork onto a second stream and join back
+    # inside the capture) and replayed on new inputs: the same as the eager build
+    c3 = torch.zeros_like(c1)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        b2d(c3, vals, None, None, dmin2, dmax2, workspace=ws)  # warm-up outside the capture
+    torch.cuda.current_stream().wait_stream(side)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        b2d(c3, vals, None, None, dmin2, dmax2, workspace=ws)
+    vals.copy_(cuda(rng.standard_normal((B1.npoints, B2.npoints, B))))
+    g.replay()
+    b2d(c1, vals, None, None, dmin2, dmax2, workspace=ws)
+    torch.cuda.synchronize()
+    assert torch.equal(c1, c3)
 
 
 @pytest.mark.parametrize("precision,rounds", [("fp64", 2), ("fp32_refine", 1), ("fp32_refine", 2)])
