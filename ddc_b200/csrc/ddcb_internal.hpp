@@ -298,6 +298,17 @@ void tune_uneven_batch(UnevenBatch& b, double const* vals, double const* dlo, do
                        double const* coords, double* out, int reps, cudaStream_t s);
 
 // tensor2d.cu
+// A second stream of the calling host thread on the current device, with the two events of a
+// fork and a join: the 2D and 3D builds run their short derivative-slab passes there, beside the
+// long value pass, and join before the passes that read them. Kept per host thread (the calls of
+// one thread are ordered), created on first use and kept until the thread ends.
+struct SideStream
+{
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+SideStream& side_stream_for_current_device();
 size_t build2d_workspace_bytes(Builder const& b1, Builder const& b2, int64_t nbatch);
 void launch_build2d(Builder const& b1, Builder const& b2, double* coefs, double const* vals, double const* dmin1,
                     double const* dmax1, double const* dmin2, double const* dmax2, double const* m11, double const* m21,

@@ -18,19 +18,6 @@
 
 namespace ddcb {
 
-namespace {
-
-// A second stream of the calling host thread on the current device, with the two events of a
-// fork and a join: the 2D build runs its dim-2 derivative slab passes there, beside the first
-// group's value pass. Kept per host thread (calls of one thread are ordered), created on first use
-// and kept until the thread ends.
-struct SideStream
-{
-    int device = -1;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr;
-};
-
 SideStream& side_stream_for_current_device()
 {
     thread_local SideStream side[16];
@@ -46,6 +33,8 @@ SideStream& side_stream_for_current_device()
     }
     return ss;
 }
+
+namespace {
 
 // Fields per group: the x1-pass result of a group stays near 40 MiB (L2-sized), and at most
 // max_group fields (0: no cap).

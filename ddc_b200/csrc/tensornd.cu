@@ -73,7 +73,14 @@ void launch_build3d(Builder const& b1, Builder const& b2, Builder const& b3, dou
     double* W1 = ws;                  // (s1, e2, e3, B)
     double* W2 = ws + s1 * e2 * e3 * B; // (s1, s2, e3, B)
     Lines const none {0, 1, 0, 0, 0};
-    // ---- pass 1: dimension 1, one build per (kind2, kind3) ----
+    // ---- pass 1: dimension 1, one build per (kind2, kind3); the derivative slabs (short launches)
+    //      on a second stream beside the values, joined before pass 2 ----
+    bool const slabs = r2.count[1] + r2.count[2] + r3.count[1] + r3.count[2] > 0;
+    SideStream* side = slabs ? &side_stream_for_current_device() : nullptr;
+    if (side) {
+        DDCB_CUDA_CHECK(cudaEventRecord(side->fork, s));
+        DDCB_CUDA_CHECK(cudaStreamWaitEvent(side->stream, side->fork, 0));
+    }
     for (int k3 = 0; k3 < 3; ++k3) {
         for (int k2 = 0; k2 < 3; ++k2) {
             int64_t const n2 = r2.count[k2], n3 = r3.count[k3];
@@ -91,8 +98,12 @@ void launch_build3d(Builder const& b1, Builder const& b2, Builder const& b3, dou
             double* out = W1 + (r2.start[k2] * e3 + r3.start[k3]) * B;
             Lines const lo {s1, e2 * e3 * B, n3 * B, n2, e3 * B};
             launch_build(b1, out, lo, v, in_lines(r1.count[0]), dlo, dlo ? in_lines(r1.count[1]) : none, dhi,
-                         dhi ? in_lines(r1.count[2]) : none, s);
+                         dhi ? in_lines(r1.count[2]) : none, (side && base != 0) ? side->stream : s);
         }
+    }
+    if (side) {
+        DDCB_CUDA_CHECK(cudaEventRecord(side->join, side->stream));
+        DDCB_CUDA_CHECK(cudaStreamWaitEvent(s, side->join, 0));
     }
     // ---- pass 2: dimension 2 of W1 (s1, e2, e3*B) -> W2 (s1, s2, e3*B) ----
     {
