@@ -322,7 +322,10 @@ ddcb_status ddcb_build2d_workspace_bytes(ddcb_builder b1, ddcb_builder b2, int64
  *   derivs_min2 / derivs_max2: (np1, nbv2, nbatch), read when b2's closure is HERMITE;
  *   mixed_* (nbv1, nbv2, nbatch): cross derivatives at the four corners, read when both are HERMITE.
  * workspace: ddcb_build2d_workspace_bytes bytes of device memory, or NULL to have the call
- * allocate it stream-ordered (cudaMallocAsync / cudaFreeAsync on `stream`). */
+ * allocate it stream-ordered (cudaMallocAsync / cudaFreeAsync on `stream`). With Hermite
+ * derivatives in dimension 2 the short derivative-slab passes run on a second stream of the
+ * calling host thread, forked from and joined back to `stream` with events: the work stays ordered
+ * on `stream`, and a capture of `stream` takes the fork and the join in. */
 ddcb_status ddcb_build2d(ddcb_builder b1, ddcb_builder b2, double* coefs, const double* vals, const double* derivs_min1,
                          const double* derivs_max1, const double* derivs_min2, const double* derivs_max2,
                          const double* mixed_min1_min2, const double* mixed_max1_min2, const double* mixed_min1_max2,
@@ -373,7 +376,8 @@ ddcb_status ddcb_build3d_workspace_bytes(ddcb_builder b1, ddcb_builder b2, ddcb_
  * [13] = min1_min2_min3, [14], [16], [17], [22], [23], [25], [26] the other corners likewise. An
  * array is read only when every dimension with a derivative kind has a HERMITE closure on that
  * side (the others may be NULL). workspace: ddcb_build3d_workspace_bytes bytes of device memory,
- * or NULL to have the call allocate it stream-ordered. */
+ * or NULL to have the call allocate it stream-ordered. The dimension-1 derivative-slab passes
+ * run on a second stream of the calling thread, forked and joined as in ddcb_build2d. */
 ddcb_status ddcb_build3d(ddcb_builder b1, ddcb_builder b2, ddcb_builder b3, double* coefs, const double* const* inputs,
                          int64_t nbatch, void* workspace, uint64_t workspace_bytes, ddcb_stream stream);
 
