@@ -353,11 +353,18 @@ def measure_configs(peak, reps):
     ms_l2 = _time_ms(step, 10 * reps, 1)
     pts = 1000 * (1000 + 1000) / 2
     bytes_fused = 1000 * 1000 * 8 + 1000 * 1003 * 8 + 1000 * 1000 * 16
+    # the same with a builder planned for 128 chunks per line (the chunks option): a batch this
+    # small gives each SM one 8-line tile, whose 1024 threads all sweep with 128 chunks
+    b128 = D.SplineBuilder(bs, chunks=128)
+    step128 = lambda i: b128.build_and_evaluate(e, cs[i], vals[i], xs[i], ys[i])
+    ms128 = _time_ms(step128, 10 * reps, sets)
     out["periodic_cubic_1000x1000"] = {
         "schedule": "fused build+eval kernel" if fused else "two kernels",
         "ms": ms_rot, "Gpts_per_s": pts / ms_rot / 1e6, "GBps": bytes_fused / ms_rot / 1e6,
         "hbm_frac": bytes_fused / ms_rot / 1e6 / peak, "ms_l2_resident": ms_l2,
-        "note": "8 rotating buffer sets (320 MB) for the HBM figure; one set for the L2-resident one"}
+        "chunks_128": {"ms": ms128, "GBps": bytes_fused / ms128 / 1e6, "hbm_frac": bytes_fused / ms128 / 1e6 / peak},
+        "note": "8 rotating buffer sets (320 MB) for the HBM figure; one set for the L2-resident one; "
+                "default builder options, and chunks_128 with the builder option chunks=128"}
     del vals, xs, cs, ys
     # ---- non-uniform quintic Hermite, 65536 lines: FP64 vs FP32 + FP64 refinement -------------
     br = W.config2_breaks(1024)
